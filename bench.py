@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""bench.py -- exact M(10^16) on B200 (seconds per M(X)) plus batched M(X)/s.
+
+One "step" is one complete M(10^16) through the engine: segmented Mobius sieve,
+dense + compressed Mertens tables, term planning, persistent S1/S2 kernel and
+the reduction -- nothing cached between steps (the 2.5 GB table is rebuilt
+every step, so every step's working set is far larger than the 126 MB L2).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+N > 1 (torchrun, one process per GPU) runs N independent replicas: M(X) does
+not need a collective.  Rank 0 prints one JSON line.  The reference arm times
+the reference's own CPU engine (oracle/_ref, built from its sources) on this
+host's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "deleglise-rivat_b200"))
+
+X_HEADLINE = 10**16
+M_HEADLINE = -3195437  # test_cuda.cu:59
+BATCH_SEED = 20261203
+
+
+def batch_inputs(n=256, seed=BATCH_SEED):
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    return [int(round(10**u)) for u in rng.uniform(9.0, 14.0, size=n)]
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            if self.thread:
+                self.thread.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for name, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(name)
+            except Exception:
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_reference_sample(seconds_budget=40.0):
+    """Reference CPU engine (oracle/_ref) on this host: one M(10^16) with all cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle_py import Reference
+
+    cores = os.cpu_count() or 1
+    if not Reference.available():
+        from oracle_py import Oracle
+
+        o = Oracle()
+        t0 = time.perf_counter()
+        m = o.mertens(10**13, cores)
+        dt = time.perf_counter() - t0
+        return {"value": dt, "unit": "s per M(10^13)", "cores": cores, "kind": "port",
+                "sample": "oracle port M(10^13), reference build absent", "M": m}
+    r = Reference()
+    r.compute_mertens(10**8, cores)  # warm-up, as the reference's benchmarks do
+    t0 = time.perf_counter()
+    m = r.compute_mertens(X_HEADLINE, cores)
+    dt = time.perf_counter() - t0
+    return {"value": dt, "unit": "s per M(10^16)", "cores": cores, "kind": "reference",
+            "sample": "one full M(10^16) by the reference engine (default env: streamed table)", "M": m}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle_py import Reference
+
+    cores = os.cpu_count() or 1
+    if not Reference.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (reference sources absent)"}))
+        return
+    r = Reference()
+    for _ in range(max(1, args.warmup)):
+        r.compute_mertens(10**8, cores)
+    times = []
+    t_start = time.perf_counter()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        m = r.compute_mertens(X_HEADLINE, cores)
+        times.append(time.perf_counter() - t0)
+        assert m == M_HEADLINE, m
+        if time.perf_counter() - t_start > 150:
+            break
+    v = statistics.median(times)
+    line = {
+        "impl": "reference", "metric": "sec per M(10^16)", "value": v, "unit": "s", "n_gpus": args.gpus,
+        "steps": len(times), "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (the single input X=10^16)",
+        "config": {"workload": "M(10^16), reference default parameters (streamed table)", "X": X_HEADLINE},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": cores, "kind": "reference",
+                         "sample": f"{len(times)} full M(10^16) runs (capped at ~150 s), median"},
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_engine(args, world, rank, local):
+    import torch
+
+    import dr_b200
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    eng = dr_b200.Engine(local, stream.cuda_stream)
+    X = X_HEADLINE
+    p = dr_b200.default_params(X, dr_b200.POLICY_REFERENCE if args.policy == "reference" else dr_b200.POLICY_GPU)
+
+    # warm-up (also the correctness gate)
+    for _ in range(args.warmup):
+        r = eng.mertens(X, p)
+        if r.M != M_HEADLINE:
+            raise SystemExit(f"M(10^16) mismatch: {r.M}")
+
+    clocks = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    host_t0 = time.perf_counter()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        r = eng.mertens(X, p)
+        stats.append(r.stats)
+        if r.M != M_HEADLINE:
+            raise SystemExit(f"M(10^16) mismatch: {r.M}")
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    host_dt = time.perf_counter() - host_t0
+    barrier(world)
+    clocks.stop()
+    dev_s = ev0.elapsed_time(ev1) / 1e3
+    dev_s = max_over_ranks(dev_s, world)
+    host_dt = max_over_ranks(host_dt, world)
+    sec_per = dev_s / args.steps
+    value = sec_per / world  # whole job: N replicas finish N results in sec_per
+
+    # phase breakdown (device events recorded by the engine on the same stream)
+    tab = statistics.mean(s.table_ms for s in stats)
+    plan = statistics.mean(s.plan_ms for s in stats)
+    sums = statistics.mean(s.sums_ms for s in stats)
+    launches = sum(s.kernel_launches for s in stats)
+
+    # batched config (256 uneven X in one table build + one persistent launch)
+    batch = None
+    if not args.no_batch:
+        xs = batch_inputs()
+        got, _ = eng.mertens_batch(xs)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        reps = 3
+        t0.record(stream)
+        for _ in range(reps):
+            got, bst = eng.mertens_batch(xs)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        bs = t0.elapsed_time(t1) / 1e3 / reps
+        # baseline: 256 sequential plain single-query calls with default parameters
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        seq = [eng.mertens(x).M for x in xs]
+        s1.record(stream)
+        torch.cuda.synchronize()
+        ss = s0.elapsed_time(s1) / 1e3
+        assert seq == got
+        batch = {"queries": len(xs), "M_per_s": len(xs) / bs, "s_per_batch": bs,
+                 "sequential_plain_M_per_s": len(xs) / ss, "speedup_vs_sequential": ss / bs,
+                 "seed": BATCH_SEED, "X": "round(10**U), U~U(9,14)"}
+
+    peak, peak_kind = load_peaks()
+    # dominant kernel: S1/S2 sums (int-bound) or the table build; algorithmic bytes
+    s0_ = stats[0]
+    table_bytes = dr_b200.table_bytes(p.u_total, p.u_dense, p.mu_limit)
+    phases = {"table_ms": tab, "plan_ms": plan, "sums_ms": sums}
+    dom = max(phases, key=phases.get)
+    if dom == "table_ms":
+        achieved = table_bytes / (tab / 1e3) / 1e9
+        kernel = "sieve_kernel+seg_scan+fixup (table build)"
+    else:
+        # S1 gathers: 2 B per dense lookup; S2: 0.5 B of wheel per position
+        alg = 2 * s0_.s1_ops + 0.5 * s0_.s2_ops
+        achieved = alg / (sums / 1e3) / 1e9
+        kernel = "sums_kernel"
+    line = {
+        "metric": "sec per M(10^16)", "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sec_per * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64", "data": "synthetic (the single input X=10^16)",
+        "config": {"workload": f"M(10^16), {args.policy} parameters", "X": X, "u_total": p.u_total,
+                   "u_dense": p.u_dense, "cx": p.cx, "mu_limit": p.mu_limit,
+                   "l2": "inputs larger than L2 (table rebuilt each step)", "parallelism": f"replicas x{world}"},
+        "phases_ms": phases,
+        "gpu_launches": launches,
+        "e2e": {"value": host_dt / args.steps / world, "unit": "s", "h2d_bytes_per_step": 48 + 4 * 8000,
+                "d2h_bytes_per_step": 40},
+        "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None},
+        "clocks": clocks.summary(),
+        "batched": batch,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_reference_sample()
+    if rank == 0:
+        print(json.dumps(line))
+    eng.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--policy", choices=["reference", "gpu"], default="reference")
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_engine(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

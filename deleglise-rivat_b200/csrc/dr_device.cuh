@@ -1,0 +1,294 @@
+// dr_device.cuh -- device helpers shared by the B200 Deleglise-Rivat kernels.
+//
+// Exact integer quotients, the mod-6 S2 summands, table lookups (dense int16
+// prefix, compressed bit planes, Mobius wheel) and the decoding of one outer
+// evaluation into its S1 / S2 index ranges.  Reference lines are cited as
+// mertens_dr.hpp:<line> (ecreeth/deleglise-rivat).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace drb {
+
+typedef unsigned long long u64;
+typedef long long i64;
+
+// ---------------------------------------------------------------------------
+// Exact floor(y / d) without floating point in the result.
+//
+// The reference divides in IEEE double when y <= 2^53 and in int64 above
+// (fast_div, mertens_dr.hpp:80-86).  Here every quotient is integer-exact:
+// an FP32 reciprocal *estimate* that never exceeds 1/d proposes a partial
+// quotient t <= floor(r/d); the integer remainder r -= t*d is then exact and
+// stays non-negative, and the loop repeats on the remainder (about 17 new
+// quotient bits per step) until r < d.  Floating point only proposes; the
+// integer arithmetic decides.
+// ---------------------------------------------------------------------------
+
+// 1/d rounded down with margin: RU conversion makes fd >= d, rcp.approx is
+// within a few ulp of 1/fd, and the (1 - 2^-17) factor absorbs that error.
+__device__ __forceinline__ float rcp_floor_estimate(uint32_t d) {
+    const float fd = __uint2float_ru(d);
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(fd));
+    return r * 0.999992370605468750f;
+}
+
+// y < 2^64, 1 <= d < 2^32, inv = rcp_floor_estimate(d).
+__device__ __forceinline__ u64 udiv_u64_u32(u64 y, uint32_t d, float inv) {
+    u64 q = 0;
+    while (y >= d) {
+        u64 t = __float2ull_rz(__fmul_rz(__ull2float_rz(y), inv));
+        t = t ? t : 1ull;
+        q += t;
+        y -= t * (u64)d;
+    }
+    return q;
+}
+
+__device__ __forceinline__ u64 udiv(u64 y, u64 d) {
+    if (d >> 32) return y / d;  // divisor above 32 bits: rare, exact library path
+    if ((y >> 32) == 0) return (uint32_t)y / (uint32_t)d;
+    return udiv_u64_u32(y, (uint32_t)d, rcp_floor_estimate((uint32_t)d));
+}
+
+// ---------------------------------------------------------------------------
+// S2 summands (mertens_dr.hpp:462-482 tabulates them; here they come from
+// their definitions).  For j coprime to 6 and q = floor(y/j), the terms of
+// j, 2j, 3j, 6j in S2(L) = sum_{m<=L} mu(m) floor(y/m) give
+//   f_L(q) = q - [2j<=L] q/2 - [3j<=L] q/3 + [6j<=L] q/6.
+// Combined pieces 1..8 are f_A(q) - f_B(floor(q/2)) (S2(y) - S2(y/2), cut at
+// B/6 A/6 B/3 A/3 B/2 A/2 B A); single pieces 9..12 are f_A(q) (cut at A/6
+// A/3 A/2 A).  Each is additive over q = 12k + r:
+//   piece(q) = piece(12) * k + piece(r),
+// so the device evaluates a*k + T[r] with T packed as 4-bit nibbles (+8).
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr i64 piece_formula(int piece, i64 q) {
+    const i64 h = q / 2, t = q / 3, f = q / 4, s = q / 6, d = q / 12;
+    switch (piece) {
+    case 1: return (q - h - t + s) - (h - f - s + d);
+    case 2: return (q - h - t + s) - (h - f - s);
+    case 3: return (q - h - t) - (h - f - s);
+    case 4: return (q - h - t) - (h - f);
+    case 5: return (q - h) - (h - f);
+    case 6: return (q - h) - h;
+    case 7: return q - h;
+    case 8: return q;
+    case 9: return q - h - t + s;
+    case 10: return q - h - t;
+    case 11: return q - h;
+    case 12: return q;
+    default: return 0;
+    }
+}
+
+struct PieceCoef {
+    i64 a;       // piece(12)
+    u64 packed;  // nibble r holds piece(r) + 8, r = 0..11
+};
+
+__host__ __device__ constexpr PieceCoef make_piece_coef(int piece) {
+    PieceCoef c{piece_formula(piece, 12), 0};
+    for (int r = 0; r < 12; ++r) c.packed |= (u64)(piece_formula(piece, r) + 8) << (4 * r);
+    return c;
+}
+
+__device__ __forceinline__ i64 piece_eval(const PieceCoef& c, u64 q) {
+    const u64 k = q / 12u;
+    const uint32_t r = (uint32_t)(q - k * 12u);
+    const int t = (int)((c.packed >> (4 * r)) & 15u) - 8;
+    return c.a * (i64)k + t;
+}
+
+// ---------------------------------------------------------------------------
+// Tables in HBM.
+//   dM[i]      = M(i + 1) as int16, 0 <= i < u_dense   (dense prefix)
+//   planes[w]  = {nonzero, negative} bits of mu over n = u_dense+1+64w .. +63
+//   ckpt[w]    = M(u_dense + 64w)                       (int32 checkpoint)
+//   wheel[g]   = mu(j) for j = 6m+1 (x: nonzero, y: negative) and j = 6m+5
+//                (z, w) with m = 32g + bit, j <= mu_limit
+// The compressed tier is the reference's format (mertens_dr.hpp:662-752:
+// two 32-byte planes + four int32 checkpoints per 256 values) with each
+// word's two plane words stored side by side, so one lookup reads one 16-byte
+// sector of planes plus one checkpoint.
+// ---------------------------------------------------------------------------
+struct TableView {
+    const int16_t* dM;
+    const ulonglong2* planes;
+    const int32_t* ckpt;
+    const uint4* wheel;
+    i64 u_dense, u_total, mu_limit;
+};
+
+__device__ __forceinline__ int32_t table_M(const TableView& t, u64 q) {
+    if (q <= (u64)t.u_dense) return q ? (int32_t)__ldg(t.dM + (q - 1)) : 0;
+    const u64 off = q - (u64)t.u_dense - 1;
+    const u64 w = off >> 6;
+    const ulonglong2 p = __ldg(t.planes + w);
+    const int32_t c = __ldg(t.ckpt + w);
+    const u64 mask = ~0ull >> (63 - (off & 63));
+    return c + __popcll(p.x & mask) - 2 * __popcll(p.y & mask);
+}
+
+// mu(j) for j coprime to 6, j <= mu_limit
+__device__ __forceinline__ int wheel_mu(const uint4* wheel, u64 j) {
+    const u64 m = j / 6u;
+    const bool five = (j - m * 6u) == 5u;
+    const uint4 w = __ldg(wheel + (m >> 5));
+    const uint32_t b = (uint32_t)(m & 31u);
+    const uint32_t nz = five ? w.z : w.x, ng = five ? w.w : w.y;
+    return ((nz >> b) & 1u) ? (((ng >> b) & 1u) ? -1 : 1) : 0;
+}
+
+// ---------------------------------------------------------------------------
+// One query of a (possibly batched) launch.
+// ---------------------------------------------------------------------------
+struct QueryDev {
+    u64 X;
+    i64 u;          // this query's S1 lower cut: n > y/u (u <= table u_total)
+    double cx;      // split parameter
+    i64 N;          // X / u
+    i64 nc;         // candidates k <= N coprime to 6
+    u64 slot_base;  // first global evaluation slot of this query
+};
+
+// Split point A = floor(cx * sqrt(y)) clamped to [1, y-1] (mertens_dr.hpp:1491-1493,
+// 1528-1533).  It is a parameter, not part of any sum: every A in range gives the
+// same M(X).  It is computed with the reference's IEEE double operations (correctly
+// rounded sqrt and product, truncation) so that intermediate S1/S2 checksums can be
+// compared with the reference at identical parameters.
+__device__ __forceinline__ i64 split_point(double cx, i64 y) {
+    i64 A = __double2ll_rz(__dmul_rn(cx, __dsqrt_rn(__ll2double_rn(y))));
+    if (A >= y) A = y - 1;
+    if (A < 1) A = 1;
+    return A;
+}
+
+// Outer candidate c -> k: 1, 5, 7, 11, ... (k coprime to 6).
+__device__ __forceinline__ i64 candidate_k(i64 c) { return 3 * c + 1 + (c & 1); }
+
+enum { EVAL_NONE = 0, EVAL_SINGLE = 1, EVAL_COMB2 = 2 };
+
+// Index ranges of one evaluation in op order: S1 segments first, then S2 pieces.
+struct EvalDesc {
+    u64 y;
+    i64 coef;       // mu(k) * (+1 first eval / -1 second eval)
+    int kind;
+    int npieces;    // 4 (single) or 8 (comb2)
+    int piece0;     // 9 (single) or 1 (comb2)
+    int nseg;       // 2 + npieces
+    i64 A, B, ky, ky2;
+    i64 s1_n0[2];
+    i64 s1_cnt[2];
+    int s1_stride[2];
+    int s1_sign[2];
+    i64 jlo[8], jhi[8];
+    i64 mcnt[8];
+    u64 total;
+};
+
+__device__ __forceinline__ i64 piece_mcount(i64 lo, i64 hi) {
+    return lo > hi ? 0 : hi / 6 - lo / 6 + 1;
+}
+
+// Decode evaluation e (0/1) of candidate c of query Q.  Follows the outer
+// reduction of mertens_dr.hpp:1470-1485, 1616-1632 and the ranges of
+// eval_single_S (:1490-1525) and eval_comb2 (:1527-1614).
+__device__ inline void decode_eval(const QueryDev& Q, const TableView& T, i64 c, int e, EvalDesc& d) {
+    d.kind = EVAL_NONE;
+    d.total = 0;
+    d.nseg = 0;
+    const i64 k = candidate_k(c);
+    if (k > Q.N) return;
+    const int muk = wheel_mu(T.wheel, (u64)k);
+    if (muk == 0) return;
+    const i64 N = Q.N;
+    int range;
+    if (k <= N / 6) range = 1;
+    else if (k <= N / 3) range = 2;
+    else if (k <= N / 2) range = 3;
+    else range = 4;
+    const u64 yk = udiv(Q.X, (u64)k);
+    u64 y, y2 = 0;
+    if (e == 0) {
+        d.coef = muk;
+        if (range <= 3) { d.kind = EVAL_COMB2; y = yk; y2 = yk / 2; }
+        else { d.kind = EVAL_SINGLE; y = yk; }
+    } else {
+        d.coef = -muk;
+        if (range == 1) { d.kind = EVAL_COMB2; y = yk / 3; y2 = yk / 6; }
+        else if (range == 2) { d.kind = EVAL_SINGLE; y = yk / 3; }
+        else return;
+    }
+    d.y = y;
+    const u64 u = (u64)Q.u;
+    if (d.kind == EVAL_SINGLE) {
+        const i64 A = split_point(Q.cx, (i64)y);
+        const i64 ky = (i64)udiv(y, (u64)(A + 1));
+        const i64 start = (i64)udiv(y, u) + 1;
+        d.A = A; d.B = 0; d.ky = ky; d.ky2 = 0;
+        d.s1_n0[0] = start; d.s1_stride[0] = 1; d.s1_sign[0] = 1;
+        d.s1_cnt[0] = ky >= start ? ky - start + 1 : 0;
+        d.s1_n0[1] = 0; d.s1_stride[1] = 2; d.s1_sign[1] = 1; d.s1_cnt[1] = 0;
+        d.npieces = 4; d.piece0 = 9;
+        const i64 a6 = A / 6, a3 = A / 3, a2 = A / 2;
+        d.jlo[0] = 1;      d.jhi[0] = a6;
+        d.jlo[1] = a6 + 1; d.jhi[1] = a3;
+        d.jlo[2] = a3 + 1; d.jhi[2] = a2;
+        d.jlo[3] = a2 + 1; d.jhi[3] = A;
+    } else {
+        const i64 A = split_point(Q.cx, (i64)y);
+        const i64 B = split_point(Q.cx, (i64)y2);
+        const i64 ky = (i64)udiv(y, (u64)(A + 1));
+        const i64 ky2 = (i64)udiv(y2, (u64)(B + 1));
+        const i64 two = 2 * ky2;
+        i64 start = (i64)udiv(y, u) + 1;
+        if ((start & 1) == 0) ++start;
+        d.A = A; d.B = B; d.ky = ky; d.ky2 = ky2;
+        d.s1_n0[0] = start; d.s1_stride[0] = 2; d.s1_sign[0] = 1;
+        d.s1_cnt[0] = ky >= start ? (ky - start) / 2 + 1 : 0;
+        // even-n correction between kappa_y and 2*kappa_{y/2} (:1568-1610)
+        i64 e0 = 0, last = -1;
+        int sg = 1;
+        if (two > ky) { e0 = ky + 1; last = two; sg = -1; }
+        else if (two < ky) { e0 = two + 1; last = ky; sg = 1; }
+        if (e0 & 1) ++e0;
+        d.s1_n0[1] = e0; d.s1_stride[1] = 2; d.s1_sign[1] = sg;
+        d.s1_cnt[1] = last >= e0 ? (last - e0) / 2 + 1 : 0;
+        d.npieces = 8; d.piece0 = 1;
+        const i64 b6 = B / 6, a6 = A / 6, b3 = B / 3, a3 = A / 3, b2 = B / 2, a2 = A / 2;
+        d.jlo[0] = 1;      d.jhi[0] = b6;
+        d.jlo[1] = b6 + 1; d.jhi[1] = a6;
+        d.jlo[2] = a6 + 1; d.jhi[2] = b3;
+        d.jlo[3] = b3 + 1; d.jhi[3] = a3;
+        d.jlo[4] = a3 + 1; d.jhi[4] = b2;
+        d.jlo[5] = b2 + 1; d.jhi[5] = a2;
+        d.jlo[6] = a2 + 1; d.jhi[6] = B;
+        d.jlo[7] = B + 1;  d.jhi[7] = A;
+    }
+    d.nseg = 2 + d.npieces;
+    u64 tot = (u64)d.s1_cnt[0] + (u64)d.s1_cnt[1];
+    for (int p = 0; p < d.npieces; ++p) {
+        d.mcnt[p] = piece_mcount(d.jlo[p], d.jhi[p]);
+        tot += (u64)d.mcnt[p];
+    }
+    d.total = tot;
+}
+
+// Constant part of an evaluation: 1 + kappa*M(A) (single) or
+// kappa_y*M(A) - kappa_y2*M(B) (comb2), mertens_dr.hpp:1524, 1613.
+__device__ __forceinline__ i64 eval_constant(const EvalDesc& d, const TableView& T) {
+    if (d.kind == EVAL_SINGLE) return 1 + d.ky * (i64)table_M(T, (u64)d.A);
+    if (d.kind == EVAL_COMB2)
+        return d.ky * (i64)table_M(T, (u64)d.A) - d.ky2 * (i64)table_M(T, (u64)d.B);
+    return 0;
+}
+
+__device__ __forceinline__ u64 warp_sum_u64(u64 v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+}  // namespace drb

@@ -1,0 +1,707 @@
+// dr_engine.cu -- host side of the B200 Deleglise-Rivat engine and its C ABI.
+//
+// One dr_ctx owns a CUDA stream and grow-only device buffers.  A query runs as
+//   table build : sieve_kernel -> seg_scan_kernel -> fixup_kernel
+//   planning    : plan_kernel (op counts, constant parts) -> u64 scan
+//   sums        : sums_kernel (persistent warps, device work queue)
+// followed by one device->host copy of the per-query {C, S1, S2} sums.
+// Nothing runs on the CPU except the parameter policy and the list of sieving
+// primes up to sqrt(u); there is no CPU fallback.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/dr_engine.h"
+#include "dr_kernels.cuh"
+#include "dr_params.hpp"
+
+using namespace drb;
+
+namespace {
+
+thread_local std::string g_err = "";
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CU(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(DR_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                                  \
+    } while (0)
+
+constexpr int64_t kDenseInt16Limit = 7600000000LL;  // |M(n)| < 32768 for n <= 7.6e9
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+double now_ms() {
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+
+struct dr_ctx {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    uint64_t budget = 0;
+    uint64_t held = 0;
+    // table buffers
+    DevBuf dM, planes, ckpt, wheel, seg_sum, seg_off, primes, stencil;
+    // query buffers
+    DevBuf queries, ops, prefix, scan_tmp, acc, counts, ticket, misc;
+    // table state
+    bool table_valid = false;
+    int64_t t_u_total = 0, t_u_dense = 0, t_mu_limit = 0, t_nwords = 0;
+    int t_S = 0;
+    // host
+    std::vector<uint32_t> host_primes;
+    int64_t host_primes_root = -1;
+    uint64_t* pinned = nullptr;  // 3 * pinned_q u64 + counts
+    size_t pinned_cap = 0;
+    std::vector<uint64_t> last_sums;
+    cudaEvent_t ev[8] = {};
+    bool sieve_attr_set = false;
+};
+
+namespace {
+
+int ensure(dr_ctx* c, DevBuf& b, size_t bytes) {
+    bytes = std::max<size_t>(bytes, 16);
+    if (bytes <= b.cap) return DR_OK;
+    const size_t rounded = (bytes + 255) & ~size_t(255);
+    if (b.p) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(b.p);
+        c->held -= b.cap;
+        b.p = nullptr;
+        b.cap = 0;
+    }
+    if (c->budget && c->held + rounded > c->budget)
+        return fail(DR_ERR_NOMEM, "device budget exceeded: need %zu more bytes, hold %llu of %llu", rounded,
+                    (unsigned long long)c->held, (unsigned long long)c->budget);
+    cudaError_t e = cudaMalloc(&b.p, rounded);
+    if (e != cudaSuccess) {
+        b.p = nullptr;
+        cudaGetLastError();
+        return fail(DR_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", rounded, cudaGetErrorString(e));
+    }
+    b.cap = rounded;
+    c->held += rounded;
+    return DR_OK;
+}
+
+void release(dr_ctx* c, DevBuf& b) {
+    if (b.p) {
+        cudaFree(b.p);
+        c->held -= b.cap;
+    }
+    b.p = nullptr;
+    b.cap = 0;
+}
+
+// Sieving primes up to root, cached per context.
+const std::vector<uint32_t>& primes_upto(dr_ctx* c, int64_t root) {
+    if (c->host_primes_root == root) return c->host_primes;
+    c->host_primes.clear();
+    if (root >= 2) {
+        std::vector<uint8_t> flag((size_t)root + 1, 1);
+        for (int64_t p = 2; p <= root; ++p) {
+            if (!flag[(size_t)p]) continue;
+            c->host_primes.push_back((uint32_t)p);
+            for (int64_t m = p * p; m <= root; m += p) flag[(size_t)m] = 0;
+        }
+    }
+    c->host_primes_root = root;
+    return c->host_primes;
+}
+
+// 4 copies of the periodic stencil shifted by 0..3 bytes (entry i describes
+// n = i + 1: weights of 2,3,5,7,11 and square flags of 4 and 9).
+std::vector<uint32_t> make_stencil4() {
+    std::vector<uint8_t> st(kStencilPeriod + 8);
+    const unsigned small[5] = {2, 3, 5, 7, 11};
+    for (int i = 0; i < kStencilPeriod + 8; ++i) {
+        const int n = (i % kStencilPeriod) + 1;
+        unsigned a = 0;
+        for (unsigned p : small)
+            if (n % (int)p == 0) a += (unsigned)((32 - __builtin_clz(p - 1)) | 1);
+        if (n % 4 == 0 || n % 9 == 0) a |= 0x80u;
+        st[(size_t)i] = (uint8_t)a;
+    }
+    std::vector<uint32_t> out((size_t)4 * kStencilWords);
+    for (int s = 0; s < 4; ++s)
+        for (int w = 0; w < kStencilWords; ++w) {
+            uint32_t v = 0;
+            for (int b = 0; b < 4; ++b) {
+                const size_t idx = (size_t)(4 * w + s + b);
+                v |= (uint32_t)(idx < st.size() ? st[idx] : 0) << (8 * b);
+            }
+            out[(size_t)s * kStencilWords + (size_t)w] = v;
+        }
+    return out;
+}
+
+int64_t num_candidates(int64_t N) {  // k <= N with gcd(k, 6) = 1
+    if (N <= 0) return 0;
+    const int64_t r = N % 6;
+    return 2 * (N / 6) + (r >= 1) + (r >= 5);
+}
+
+int64_t split_point_host(double cx, int64_t y) {
+    int64_t A = (int64_t)(cx * std::sqrt((double)y));
+    if (A >= y) A = y - 1;
+    if (A < 1) A = 1;
+    return A;
+}
+
+int pick_segment(const dr_params* p) {
+    int lg = (p && p->segment_log2) ? p->segment_log2 : 17;
+    lg = std::max(12, std::min(lg, 17));
+    return 1 << lg;
+}
+
+TableView view_of(dr_ctx* c) {
+    TableView T;
+    T.dM = (const int16_t*)c->dM.p;
+    T.planes = (const ulonglong2*)c->planes.p;
+    T.ckpt = (const int32_t*)c->ckpt.p;
+    T.wheel = (const uint4*)c->wheel.p;
+    T.u_dense = c->t_u_dense;
+    T.u_total = c->t_u_total;
+    T.mu_limit = c->t_mu_limit;
+    return T;
+}
+
+int check_table_limits(int64_t u_total, int64_t u_dense, int64_t mu_limit) {
+    if (u_total < 1) return fail(DR_ERR_PARAMS, "u_total must be >= 1 (got %lld)", (long long)u_total);
+    if (u_dense < 0 || u_dense > u_total)
+        return fail(DR_ERR_PARAMS, "u_dense must be in [0, u_total] (got %lld)", (long long)u_dense);
+    if (u_dense > kDenseInt16Limit)
+        return fail(DR_ERR_PARAMS, "u_dense %lld exceeds the int16 prefix range (7.6e9)", (long long)u_dense);
+    if (mu_limit < 0 || mu_limit > u_total)
+        return fail(DR_ERR_PARAMS, "mu_limit must be in [0, u_total] (got %lld)", (long long)mu_limit);
+    if (u_total > (int64_t)4000000000000LL) return fail(DR_ERR_PARAMS, "u_total above 4e12 is not supported");
+    return DR_OK;
+}
+
+int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, const dr_params* tuning,
+                dr_stats* st) {
+    int rc = check_table_limits(u_total, u_dense, mu_limit);
+    if (rc) return rc;
+    const int S = pick_segment(tuning);
+    const int block = (tuning && tuning->block_threads) ? tuning->block_threads : 1024;
+    if (block < 128 || block > 1024 || (block & 31))
+        return fail(DR_ERR_PARAMS, "block_threads must be a multiple of 32 in [128, 1024]");
+    const int64_t comp = u_total - u_dense;
+    const int64_t dense_segs = (u_dense + S - 1) / S;
+    const int64_t comp_segs = (comp + S - 1) / S;
+    const int64_t nseg = dense_segs + comp_segs;
+    const int64_t nwords = (comp + 63) / 64;
+    const int64_t wheel_groups = mu_limit / 192 + 2;
+    if ((rc = ensure(c, c->dM, (size_t)u_dense * 2 + 64))) return rc;
+    if ((rc = ensure(c, c->planes, (size_t)nwords * 16))) return rc;
+    if ((rc = ensure(c, c->ckpt, (size_t)nwords * 4))) return rc;
+    if ((rc = ensure(c, c->wheel, (size_t)wheel_groups * 16))) return rc;
+    if ((rc = ensure(c, c->seg_sum, (size_t)nseg * 4))) return rc;
+    if ((rc = ensure(c, c->seg_off, (size_t)nseg * 4))) return rc;
+    const std::vector<uint32_t>& pr = primes_upto(c, isqrt_i64(u_total));
+    if ((rc = ensure(c, c->primes, pr.size() * 4))) return rc;
+    if (!pr.empty()) CU(cudaMemcpyAsync(c->primes.p, pr.data(), pr.size() * 4, cudaMemcpyHostToDevice, c->stream));
+
+    SieveArgs a;
+    a.u_total = u_total;
+    a.u_dense = u_dense;
+    a.mu_limit = mu_limit;
+    a.dense_segs = dense_segs;
+    a.nseg = nseg;
+    a.S = S;
+    a.n_primes = (int)pr.size();
+    auto first_at_least = [&](uint32_t v) {
+        return (int)(std::lower_bound(pr.begin(), pr.end(), v) - pr.begin());
+    };
+    a.sq_first = first_at_least(5);
+    a.w_first = first_at_least(13);
+    a.tierB_first = std::max(a.w_first, first_at_least((uint32_t)std::max(13, S / 64)));
+    a.primes = (const uint32_t*)c->primes.p;
+    a.stencil4 = (const uint32_t*)c->stencil.p;
+    a.dM = (int16_t*)c->dM.p;
+    a.planes = (ulonglong2*)c->planes.p;
+    a.ckpt = (int32_t*)c->ckpt.p;
+    a.wheel = (uint4*)c->wheel.p;
+    a.seg_sum = (int32_t*)c->seg_sum.p;
+
+    const size_t smem = sieve_smem_bytes(S);
+    int per_sm = 0;
+    sieve_kernel_attrs(smem, block, &per_sm);
+    if (per_sm < 1) per_sm = 1;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(nseg, (int64_t)c->sm_count * per_sm));
+
+    CU(cudaEventRecord(c->ev[0], c->stream));
+    CU(cudaMemsetAsync(c->wheel.p, 0, (size_t)wheel_groups * 16, c->stream));
+    launch_sieve(a, grid, block, smem, c->stream);
+    CU(cudaGetLastError());
+    launch_seg_scan((const int32_t*)c->seg_sum.p, (int32_t*)c->seg_off.p, nseg, c->stream);
+    CU(cudaGetLastError());
+    launch_fixup((int16_t*)c->dM.p, u_dense, S, (const int32_t*)c->seg_off.p, (int32_t*)c->ckpt.p, nwords,
+                 dense_segs, c->sm_count, c->stream);
+    CU(cudaGetLastError());
+    CU(cudaEventRecord(c->ev[1], c->stream));
+
+    c->table_valid = true;
+    c->t_u_total = u_total;
+    c->t_u_dense = u_dense;
+    c->t_mu_limit = mu_limit;
+    c->t_nwords = nwords;
+    c->t_S = S;
+    if (st) {
+        st->sieve_launches += 1;
+        st->kernel_launches += 3;
+    }
+    return DR_OK;
+}
+
+// Endpoint-coverage check of one query against table limits.
+int check_query(int64_t X, const dr_params& p, int64_t t_u_total, int64_t t_mu_limit) {
+    if (X < 1) return DR_OK;
+    if (!(p.cx > 0.0) || !(p.cx < 64.0)) return fail(DR_ERR_PARAMS, "cx must be in (0, 64)");
+    if (p.u_total < 1 || p.u_total > t_u_total) return fail(DR_ERR_PARAMS, "query u exceeds table u_total");
+    if (X <= t_u_total) return DR_OK;  // answered from the table
+    const int64_t N = X / p.u_total;
+    if (N > t_mu_limit)
+        return fail(DR_ERR_PARAMS, "N = X/u = %lld exceeds mu_limit %lld", (long long)N, (long long)t_mu_limit);
+    const int64_t A = split_point_host(p.cx, X);
+    if (A > t_mu_limit)
+        return fail(DR_ERR_PARAMS, "endpoint A = %lld exceeds mu_limit %lld", (long long)A, (long long)t_mu_limit);
+    if (A > t_u_total) return fail(DR_ERR_PARAMS, "endpoint A exceeds u_total");
+    return DR_OK;
+}
+
+int resolve_params(int64_t X, const dr_params* in, dr_params* out) {
+    if (in) {
+        *out = *in;
+        return DR_OK;
+    }
+    return dr_default_params(X, DR_POLICY_REFERENCE, out);
+}
+
+// Run a batch of queries on the current table (already built).
+int run_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, int64_t* out, dr_stats* st,
+                const dr_params* tuning) {
+    int rc;
+    std::vector<QueryDev> qs((size_t)nq);
+    u64 slots = 0;
+    for (int64_t i = 0; i < nq; ++i) {
+        QueryDev& q = qs[(size_t)i];
+        q.X = (u64)std::max<int64_t>(X[i], 0);
+        q.u = P[i].u_total;
+        q.cx = P[i].cx;
+        q.N = (X[i] <= c->t_u_total) ? 0 : X[i] / P[i].u_total;
+        q.nc = num_candidates(q.N);
+        q.slot_base = slots;
+        slots += 2 * (u64)q.nc;
+    }
+    if ((rc = ensure(c, c->queries, (size_t)nq * sizeof(QueryDev)))) return rc;
+    if ((rc = ensure(c, c->acc, (size_t)nq * 3 * 8))) return rc;
+    if ((rc = ensure(c, c->counts, (size_t)nq * 4 * 8))) return rc;
+    if ((rc = ensure(c, c->ops, (size_t)std::max<u64>(slots, 1) * 8))) return rc;
+    if ((rc = ensure(c, c->prefix, (size_t)(slots + 1) * 8))) return rc;
+    if ((rc = ensure(c, c->scan_tmp, scan_u64_tmp_elems(slots) * 8))) return rc;
+    if ((rc = ensure(c, c->ticket, 8))) return rc;
+    const size_t need_pinned = (size_t)nq * 7;
+    if (c->pinned_cap < need_pinned) {
+        if (c->pinned) cudaFreeHost(c->pinned);
+        c->pinned = nullptr;
+        CU(cudaMallocHost((void**)&c->pinned, need_pinned * 8));
+        c->pinned_cap = need_pinned;
+    }
+    const TableView T = view_of(c);
+    const int qn = (int)nq;
+    CU(cudaEventRecord(c->ev[2], c->stream));
+    CU(cudaMemcpyAsync(c->queries.p, qs.data(), (size_t)nq * sizeof(QueryDev), cudaMemcpyHostToDevice, c->stream));
+    CU(cudaMemsetAsync(c->acc.p, 0, (size_t)nq * 3 * 8, c->stream));
+    CU(cudaMemsetAsync(c->counts.p, 0, (size_t)nq * 4 * 8, c->stream));
+    CU(cudaMemsetAsync(c->ticket.p, 0, 8, c->stream));
+    launch_direct((const QueryDev*)c->queries.p, qn, T, (u64*)c->acc.p, c->stream);
+    int launches = 1;
+    if (slots > 0) {
+        launch_plan((const QueryDev*)c->queries.p, qn, T, slots, (u64*)c->ops.p, (u64*)c->acc.p, (i64*)c->counts.p,
+                    c->sm_count, c->stream);
+        launch_scan_u64((const u64*)c->ops.p, (u64*)c->prefix.p, slots, (u64*)c->scan_tmp.p,
+                        scan_u64_tmp_elems(slots), c->stream);
+        launches += 4;
+    }
+    CU(cudaGetLastError());
+    CU(cudaEventRecord(c->ev[3], c->stream));
+    if (slots > 0) {
+        SumsArgs sa;
+        sa.queries = (const QueryDev*)c->queries.p;
+        sa.nq = qn;
+        sa.T = T;
+        sa.n_slots = slots;
+        sa.prefix = (const u64*)c->prefix.p;
+        sa.ticket = (u64*)c->ticket.p;
+        sa.acc = (u64*)c->acc.p;
+        sa.chunk_log2 = tuning ? tuning->chunk_log2 : 0;
+        int per_sm = 0;
+        sums_kernel_occupancy(256, &per_sm);
+        const int grid = c->sm_count * std::max(1, per_sm);
+        launch_sums(sa, grid, 256, c->stream);
+        CU(cudaGetLastError());
+        launches += 1;
+        if (st) st->sums_launches += 1;
+    }
+    CU(cudaEventRecord(c->ev[4], c->stream));
+    CU(cudaMemcpyAsync(c->pinned, c->acc.p, (size_t)nq * 3 * 8, cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaMemcpyAsync(c->pinned + (size_t)nq * 3, c->counts.p, (size_t)nq * 4 * 8, cudaMemcpyDeviceToHost,
+                       c->stream));
+    CU(cudaEventRecord(c->ev[5], c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    CU(cudaGetLastError());
+    c->last_sums.assign(c->pinned, c->pinned + (size_t)nq * 3);
+    for (int64_t i = 0; i < nq; ++i) {
+        const uint64_t* a = c->pinned + 3 * i;
+        out[i] = X[i] < 1 ? 0 : (int64_t)(a[0] - a[1] - a[2]);
+    }
+    if (st) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
+        st->plan_ms += ms;
+        cudaEventElapsedTime(&ms, c->ev[3], c->ev[4]);
+        st->sums_ms += ms;
+        cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]);
+        st->d2h_ms += ms;
+        st->kernel_launches += launches;
+        const uint64_t* cnt = c->pinned + (size_t)nq * 3;
+        for (int64_t i = 0; i < nq; ++i) {
+            st->terms += (int64_t)cnt[4 * i + 0];
+            st->evals += (int64_t)cnt[4 * i + 1];
+            st->s1_ops += cnt[4 * i + 2];
+            st->s2_ops += cnt[4 * i + 3];
+        }
+        if (nq == 1) {
+            st->C = c->pinned[0];
+            st->S1 = c->pinned[1];
+            st->S2 = c->pinned[2];
+            st->M = out[0];
+        }
+    }
+    return DR_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* dr_last_error(void) { return g_err.c_str(); }
+
+int dr_device_info(int device, int* sm_count, uint64_t* hbm_bytes) {
+    cudaDeviceProp prop;
+    CU(cudaGetDeviceProperties(&prop, device));
+    if (sm_count) *sm_count = prop.multiProcessorCount;
+    if (hbm_bytes) *hbm_bytes = prop.totalGlobalMem;
+    return DR_OK;
+}
+
+int dr_ctx_create(int device, void* cuda_stream, dr_ctx** out) {
+    if (!out) return fail(DR_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    CU(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(DR_ERR_ARG, "device %d out of range (%d devices)", device, ndev);
+    CU(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CU(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10)
+        return fail(DR_ERR_DEVICE, "device %d is sm_%d%d; this library is built for sm_100a", device, prop.major,
+                    prop.minor);
+    dr_ctx* c = new dr_ctx();
+    c->device = device;
+    c->sm_count = prop.multiProcessorCount;
+    if (cuda_stream) {
+        c->stream = (cudaStream_t)cuda_stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete c;
+            return fail(DR_ERR_CUDA, "cudaStreamCreate failed");
+        }
+        c->own_stream = true;
+    }
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    c->budget = (uint64_t)((double)free_b * 0.92);
+    for (auto& e : c->ev) cudaEventCreate(&e);
+    init_piece_constants();
+    std::vector<uint32_t> st = make_stencil4();
+    int rc = ensure(c, c->stencil, st.size() * 4);
+    if (rc) {
+        dr_ctx_destroy(c);
+        return rc;
+    }
+    cudaMemcpy(c->stencil.p, st.data(), st.size() * 4, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        dr_ctx_destroy(c);
+        return fail(DR_ERR_CUDA, "context init failed: %s", cudaGetErrorString(e));
+    }
+    *out = c;
+    return DR_OK;
+}
+
+int dr_ctx_destroy(dr_ctx* c) {
+    if (!c) return DR_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    DevBuf* bufs[] = {&c->dM, &c->planes, &c->ckpt, &c->wheel, &c->seg_sum, &c->seg_off, &c->primes, &c->stencil,
+                      &c->queries, &c->ops, &c->prefix, &c->scan_tmp, &c->acc, &c->counts, &c->ticket, &c->misc};
+    for (DevBuf* b : bufs) release(c, *b);
+    if (c->pinned) cudaFreeHost(c->pinned);
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return DR_OK;
+}
+
+int dr_ctx_set_hbm_budget(dr_ctx* c, uint64_t bytes) {
+    if (!c) return fail(DR_ERR_ARG, "ctx is NULL");
+    if (bytes == 0) {
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        bytes = (uint64_t)((double)(free_b + c->held) * 0.92);
+    }
+    c->budget = bytes;
+    return DR_OK;
+}
+
+int dr_default_params(int64_t X, int policy, dr_params* out) {
+    if (!out) return fail(DR_ERR_ARG, "out is NULL");
+    params_clear(out);
+    if (X < 1) {
+        out->cx = ref_choose_cx(X);
+        return DR_OK;
+    }
+    switch (policy) {
+    case DR_POLICY_REFERENCE:
+        if (ref_use_compressed(X)) ref_compressed_params(X, out);
+        else ref_dense_params(X, out);
+        return DR_OK;
+    case DR_POLICY_DENSE: ref_dense_params(X, out); return DR_OK;
+    case DR_POLICY_COMPRESSED:
+        if (X <= 100000LL) ref_dense_params(X, out);
+        else ref_compressed_params(X, out);
+        return DR_OK;
+    case DR_POLICY_GPU:
+        if (X <= 100000LL) ref_dense_params(X, out);
+        else ref_compressed_params(X, out);
+        return DR_OK;
+    }
+    return fail(DR_ERR_ARG, "unknown policy %d", policy);
+}
+
+uint64_t dr_table_bytes(int64_t u_total, int64_t u_dense, int64_t mu_limit) {
+    const int64_t comp = std::max<int64_t>(0, u_total - u_dense);
+    const int64_t nwords = (comp + 63) / 64;
+    const int64_t nseg = (u_total + 4095) / 4096 + 2;
+    return (uint64_t)u_dense * 2 + (uint64_t)nwords * 20 + (uint64_t)(mu_limit / 192 + 2) * 16 + (uint64_t)nseg * 8;
+}
+
+int dr_check_params(int64_t X, const dr_params* p, uint64_t hbm_budget) {
+    if (!p) return fail(DR_ERR_ARG, "params is NULL");
+    if (X < 1) return DR_OK;
+    int rc = check_table_limits(p->u_total, p->u_dense, p->mu_limit);
+    if (rc) return rc;
+    if ((rc = check_query(X, *p, p->u_total, p->mu_limit))) return rc;
+    if (hbm_budget && dr_table_bytes(p->u_total, p->u_dense, p->mu_limit) > hbm_budget)
+        return fail(DR_ERR_NOMEM, "table needs %llu bytes, budget %llu",
+                    (unsigned long long)dr_table_bytes(p->u_total, p->u_dense, p->mu_limit),
+                    (unsigned long long)hbm_budget);
+    return DR_OK;
+}
+
+int dr_table_build(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, const dr_params* tuning,
+                   dr_stats* st) {
+    if (!c) return fail(DR_ERR_ARG, "ctx is NULL");
+    CU(cudaSetDevice(c->device));
+    const double t0 = now_ms();
+    int rc = build_table(c, u_total, u_dense, mu_limit, tuning, st);
+    if (rc) return rc;
+    CU(cudaStreamSynchronize(c->stream));
+    if (st) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+        st->table_ms += ms;
+        st->total_ms += now_ms() - t0;
+    }
+    return DR_OK;
+}
+
+int dr_mertens(dr_ctx* c, int64_t X, const dr_params* p, int64_t* out, dr_stats* st) {
+    return dr_mertens_batch(c, &X, 1, p, out, st);
+}
+
+int dr_mertens_batch(dr_ctx* c, const int64_t* X, int64_t count, const dr_params* p, int64_t* out, dr_stats* st) {
+    if (!c || !X || !out) return fail(DR_ERR_ARG, "NULL argument");
+    if (count < 1 || count > (1 << 20)) return fail(DR_ERR_ARG, "count must be in [1, 2^20]");
+    CU(cudaSetDevice(c->device));
+    const double t0 = now_ms();
+    if (st) std::memset(st, 0, sizeof(*st));
+    std::vector<dr_params> P((size_t)count);
+    int64_t ut = 1, ud = 0, ml = 0;
+    bool any = false;
+    for (int64_t i = 0; i < count; ++i) {
+        int rc = resolve_params(X[i], p ? p + i : nullptr, &P[(size_t)i]);
+        if (rc) return rc;
+        if (X[i] < 1) continue;
+        any = true;
+        rc = check_table_limits(P[i].u_total, P[i].u_dense, P[i].mu_limit);
+        if (rc) return rc;
+        ut = std::max(ut, P[i].u_total);
+        ud = std::max(ud, P[i].u_dense);
+        ml = std::max(ml, P[i].mu_limit);
+    }
+    if (!any) {
+        for (int64_t i = 0; i < count; ++i) out[i] = 0;
+        return DR_OK;
+    }
+    for (int64_t i = 0; i < count; ++i) {
+        if (X[i] < 1) continue;
+        int rc = check_query(X[i], P[(size_t)i], ut, ml);
+        if (rc) return rc;
+    }
+    int rc = build_table(c, ut, ud, ml, p ? p : nullptr, st);
+    if (rc) return rc;
+    rc = run_queries(c, X, P.data(), count, out, st, p ? p : nullptr);
+    if (rc) return rc;
+    if (st) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+        st->table_ms += ms;
+        st->total_ms = now_ms() - t0;
+        if (count == 1) st->M = out[0];
+    }
+    return DR_OK;
+}
+
+int dr_batch_checksums(dr_ctx* c, uint64_t* out3, int64_t count) {
+    if (!c || !out3) return fail(DR_ERR_ARG, "NULL argument");
+    if ((size_t)count * 3 > c->last_sums.size()) return fail(DR_ERR_ARG, "count exceeds the last batch");
+    std::memcpy(out3, c->last_sums.data(), (size_t)count * 3 * 8);
+    return DR_OK;
+}
+
+int dr_table_read(dr_ctx* c, int64_t first, int64_t count, int32_t* M, int8_t* mu) {
+    if (!c) return fail(DR_ERR_ARG, "ctx is NULL");
+    if (!c->table_valid) return fail(DR_ERR_ARG, "no table built");
+    if (count < 0) return fail(DR_ERR_ARG, "negative count");
+    if (count == 0) return DR_OK;
+    CU(cudaSetDevice(c->device));
+    int rc = ensure(c, c->misc, (size_t)count * 6);
+    if (rc) return rc;
+    int32_t* dM = (int32_t*)c->misc.p;
+    int8_t* dmu = (int8_t*)((char*)c->misc.p + (size_t)count * 4);
+    launch_table_read(view_of(c), first, count, M ? dM : nullptr, mu ? dmu : nullptr, nullptr, c->stream);
+    CU(cudaGetLastError());
+    if (M) CU(cudaMemcpyAsync(M, dM, (size_t)count * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (mu) CU(cudaMemcpyAsync(mu, dmu, (size_t)count, cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return DR_OK;
+}
+
+// Mobius values as stored in the wheel (0 for n sharing a factor with 6).
+int dr_table_read_wheel(dr_ctx* c, int64_t first, int64_t count, int8_t* mu) {
+    if (!c || !mu) return fail(DR_ERR_ARG, "NULL argument");
+    if (!c->table_valid) return fail(DR_ERR_ARG, "no table built");
+    if (count <= 0) return DR_OK;
+    CU(cudaSetDevice(c->device));
+    int rc = ensure(c, c->misc, (size_t)count);
+    if (rc) return rc;
+    launch_table_read(view_of(c), first, count, nullptr, nullptr, (int8_t*)c->misc.p, c->stream);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(mu, c->misc.p, (size_t)count, cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return DR_OK;
+}
+
+int dr_table_checksums(dr_ctx* c, dr_table_sums* out) {
+    if (!c || !out) return fail(DR_ERR_ARG, "NULL argument");
+    if (!c->table_valid) return fail(DR_ERR_ARG, "no table built");
+    CU(cudaSetDevice(c->device));
+    int rc = ensure(c, c->misc, 64);
+    if (rc) return rc;
+    CU(cudaMemsetAsync(c->misc.p, 0, 48, c->stream));
+    launch_table_sums(view_of(c), c->t_nwords, (u64*)c->misc.p, c->sm_count, c->stream);
+    CU(cudaGetLastError());
+    uint64_t h[6];
+    CU(cudaMemcpyAsync(h, c->misc.p, 48, cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    out->dense_sum = h[0];
+    out->dense_wsum = h[1];
+    out->mu_wsum = h[2];
+    out->nz_wsum = h[3];
+    out->neg_wsum = h[4];
+    out->ckpt_wsum = h[5];
+    return DR_OK;
+}
+
+int dr_debug_udiv(dr_ctx* c, const uint64_t* y, const uint64_t* d, int64_t n, uint64_t* q) {
+    if (!c || !y || !d || !q || n < 0) return fail(DR_ERR_ARG, "bad argument");
+    if (n == 0) return DR_OK;
+    CU(cudaSetDevice(c->device));
+    int rc = ensure(c, c->misc, (size_t)n * 24);
+    if (rc) return rc;
+    u64* dy = (u64*)c->misc.p;
+    u64* dd = dy + n;
+    u64* dq = dd + n;
+    CU(cudaMemcpyAsync(dy, y, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream));
+    CU(cudaMemcpyAsync(dd, d, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream));
+    launch_debug_udiv(dy, dd, dq, n, c->stream);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(q, dq, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return DR_OK;
+}
+
+int dr_debug_piece(dr_ctx* c, const int32_t* piece, const uint64_t* q, int64_t n, int64_t* out) {
+    if (!c || !piece || !q || !out || n < 0) return fail(DR_ERR_ARG, "bad argument");
+    if (n == 0) return DR_OK;
+    CU(cudaSetDevice(c->device));
+    int rc = ensure(c, c->misc, (size_t)n * 20);
+    if (rc) return rc;
+    u64* dq = (u64*)c->misc.p;
+    i64* dout = (i64*)(dq + n);
+    int32_t* dp = (int32_t*)(dout + n);
+    CU(cudaMemcpyAsync(dq, q, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream));
+    CU(cudaMemcpyAsync(dp, piece, (size_t)n * 4, cudaMemcpyHostToDevice, c->stream));
+    launch_debug_piece(dp, dq, dout, n, c->stream);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(out, dout, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return DR_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,685 @@
+// dr_kernels.cu -- sm_100a kernels of the Deleglise-Rivat Mertens engine.
+//
+//  sieve_kernel      segmented byte-log Mobius sieve in shared memory and the
+//                    three table outputs of each segment: dense int16 prefix,
+//                    compressed bit planes + checkpoints, Mobius wheel bits
+//                    (mertens_dr.hpp:755-883 for the streamed builder,
+//                    :180-296 / :300-368 for the dense one)
+//  seg_scan_kernel   exclusive scan of per-segment Mobius sums
+//  fixup_kernel      global offsets into the dense prefix and checkpoints
+//                    (mertens_dr.hpp:884-900)
+//  plan_kernel       one thread per outer evaluation slot: op counts and the
+//                    constant part kappa*M(A) ... (mertens_dr.hpp:1470-1485)
+//  scan_u64 kernels  op-count prefix (the flattened work space)
+//  sums_kernel       persistent warps pull fixed-size chunks of the flattened
+//                    S1/S2 index space from a device work queue
+//                    (mertens_dr.hpp:1490-1632)
+#include "dr_kernels.cuh"
+
+#include <algorithm>
+
+namespace drb {
+
+__constant__ PieceCoef c_piece[13];
+
+void init_piece_constants() {
+    PieceCoef h[13];
+    for (int p = 0; p < 13; ++p) h[p] = make_piece_coef(p);
+    cudaMemcpyToSymbol(c_piece, h, sizeof(h));
+}
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t umod_u64_u32(u64 y, uint32_t d) {
+    if ((y >> 32) == 0) return (uint32_t)y % d;
+    const u64 q = udiv_u64_u32(y, d, rcp_floor_estimate(d));
+    return (uint32_t)(y - q * d);
+}
+
+__device__ __forceinline__ int warp_incl_scan(int v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// Exclusive scan of a[0..n) in shared memory; returns the total.  wtot holds
+// 33 ints of scratch.  Every thread of the block must call it.
+__device__ int block_excl_scan(int32_t* a, int n, int32_t* wtot) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int ntiles = (n + 31) >> 5;
+    const int tpw = (ntiles + nwarps - 1) / nwarps;
+    const int t0 = warp * tpw, t1 = min(ntiles, t0 + tpw);
+    int carry = 0;
+    for (int t = t0; t < t1; ++t) {
+        const int idx = (t << 5) + lane;
+        const int v = idx < n ? a[idx] : 0;
+        const int x = warp_incl_scan(v, lane);
+        if (idx < n) a[idx] = carry + x - v;
+        carry += __shfl_sync(0xffffffffu, x, 31);
+    }
+    if (lane == 0) wtot[warp] = carry;
+    __syncthreads();
+    if (warp == 0) {
+        const int v = lane < nwarps ? wtot[lane] : 0;
+        const int x = warp_incl_scan(v, lane);
+        wtot[lane] = x - v;
+        if (lane == 31) wtot[32] = x;
+    }
+    __syncthreads();
+    const int off = wtot[warp];
+    for (int t = t0; t < t1; ++t) {
+        const int idx = (t << 5) + lane;
+        if (idx < n) a[idx] += off;
+    }
+    const int total = wtot[32];
+    __syncthreads();
+    return total;
+}
+
+// Byte-log rule (mertens_dr.hpp:145-171) for value n with accumulator acc.
+__device__ __forceinline__ uint32_t finalize_byte(uint32_t acc, u64 n) {
+    if (n <= 2) return n == 1 ? 1u : (n == 2 ? 0xFFu : 0u);  // explicit 1 and 2 (:838-839)
+    if (acc & 0x80u) return 0u;
+    const uint32_t bits = 64u - __clzll(n);
+    const bool sieved_all = acc > bits - 1;
+    const bool odd = acc & 1u;
+    // sign = (-1)^acc when every factor was sieved, else the opposite sign
+    return (odd == sieved_all) ? 0xFFu : 1u;
+}
+
+size_t sieve_smem_bytes(int S) { return (size_t)S + (size_t)(S / 16) * 4 + 64; }
+
+// ---------------------------------------------------------------------------
+// Segmented byte-log Mobius sieve + table outputs.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint8_t* buf = smem;
+    uint32_t* buf32 = reinterpret_cast<uint32_t*>(smem);
+    int32_t* gs = reinterpret_cast<int32_t*>(smem + a.S);
+    __shared__ int32_t wtot[33];
+
+    const int T = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = T >> 5;
+
+    for (i64 seg = blockIdx.x; seg < a.nseg; seg += gridDim.x) {
+        const bool dense = seg < a.dense_segs;
+        const i64 base = dense ? seg * (i64)a.S : a.u_dense + (seg - a.dense_segs) * (i64)a.S;
+        const i64 end = min(base + (i64)a.S, dense ? a.u_dense : a.u_total);
+        const int len = (int)(end - base);
+        const i64 low = base + 1;
+        const int ng = (len + 15) >> 4;  // 16-value groups
+        const int nw16 = ng * 4;         // words covering the groups
+
+        // 1. periodic stencil: weights of 2,3,5,7,11 and flags of 4, 9 (:818-823)
+        {
+            const uint32_t ph0 = (uint32_t)(base % kStencilPeriod);
+            for (int i = tid; i < nw16; i += T) {
+                uint32_t ph = ph0 + 4u * (uint32_t)i;
+                ph %= (uint32_t)kStencilPeriod;
+                buf32[i] = __ldg(a.stencil4 + (ph & 3u) * kStencilWords + (ph >> 2));
+            }
+        }
+        __syncthreads();
+
+        // 2. square flags for p >= 5 (:824-829); idempotent OR, so order-free
+        for (int i = a.sq_first + tid; i < a.n_primes; i += T) {
+            const u64 p = a.primes[i];
+            const u64 sq = p * p;
+            if (sq > (u64)end) break;
+            u64 r;
+            if (sq >> 32) r = (u64)low % sq;
+            else r = umod_u64_u32((u64)low, (uint32_t)sq);
+            for (u64 j = r ? sq - r : 0; j < (u64)len; j += sq)
+                atomicOr(&buf32[j >> 2], 0x80u << ((j & 3) * 8));
+        }
+        // 3. log weights for p >= 13 (:830-835).  The byte sum stays below 0x80,
+        //    so a 32-bit add of w << 8*(j&3) never carries into a neighbour.
+        for (int i = a.w_first + warp; i < a.tierB_first; i += nwarps) {
+            const uint32_t p = a.primes[i];
+            const uint32_t w = (32u - __clz(p - 1)) | 1u;
+            const uint32_t r = umod_u64_u32((u64)low, p);
+            const uint32_t first = r ? p - r : 0;
+            for (uint32_t j = first + lane * p; j < (uint32_t)len; j += 32u * p)
+                atomicAdd(&buf32[j >> 2], w << ((j & 3) * 8));
+        }
+        for (int i = a.tierB_first + tid; i < a.n_primes; i += T) {
+            const uint32_t p = a.primes[i];
+            const uint32_t w = (32u - __clz(p - 1)) | 1u;
+            const uint32_t r = umod_u64_u32((u64)low, p);
+            for (uint32_t j = r ? p - r : 0; j < (uint32_t)len; j += p)
+                atomicAdd(&buf32[j >> 2], w << ((j & 3) * 8));
+        }
+        __syncthreads();
+
+        // 4. finalize to mu bytes in place; bytes past len become 0
+        for (int i = tid; i < nw16; i += T) {
+            const uint32_t v = buf32[i];
+            uint32_t o = 0;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int idx = 4 * i + b;
+                if (idx < len) o |= finalize_byte((v >> (8 * b)) & 0xFFu, (u64)(low + idx)) << (8 * b);
+            }
+            buf32[i] = o;
+        }
+        __syncthreads();
+
+        // 5. 16-value group sums and their exclusive scan
+        for (int g = tid; g < ng; g += T) {
+            const uint4 v = reinterpret_cast<const uint4*>(buf)[g];
+            int s = __dp4a((int)v.x, 0x01010101, 0);
+            s = __dp4a((int)v.y, 0x01010101, s);
+            s = __dp4a((int)v.z, 0x01010101, s);
+            s = __dp4a((int)v.w, 0x01010101, s);
+            gs[g] = s;
+        }
+        __syncthreads();
+        const int total = block_excl_scan(gs, ng, wtot);
+
+        // 6. outputs
+        if (dense) {
+            // dM[i] = M(i+1) local to the segment; offsets added by fixup_kernel
+            int16_t* out = a.dM + base;
+            for (int g = tid; g < ng; g += T) {
+                const uint4 v = reinterpret_cast<const uint4*>(buf)[g];
+                int run = gs[g];
+                uint32_t pk[8];
+                const uint32_t words[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int b = 0; b < 16; b += 2) {
+                    run += (int)(int8_t)((words[b >> 2] >> (8 * (b & 3))) & 0xFFu);
+                    const uint32_t lo = (uint32_t)(run & 0xFFFF);
+                    run += (int)(int8_t)((words[(b + 1) >> 2] >> (8 * ((b + 1) & 3))) & 0xFFu);
+                    pk[b >> 1] = lo | ((uint32_t)(run & 0xFFFF) << 16);
+                }
+                if (16 * g + 16 <= len) {
+                    uint4* dst = reinterpret_cast<uint4*>(out + 16 * g);
+                    dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                    dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+                } else {
+                    for (int b = 0; b < len - 16 * g; ++b)
+                        out[16 * g + b] = (int16_t)((pk[b >> 1] >> (16 * (b & 1))) & 0xFFFFu);
+                }
+            }
+        } else {
+            // 64-value words: nonzero / negative planes by ballot, local checkpoint
+            const i64 wbase = (base - a.u_dense) >> 6;
+            const int nwords = (len + 63) >> 6;
+            for (int w = warp; w < nwords; w += nwarps) {
+                const int i0 = 64 * w + lane, i1 = i0 + 32;
+                const int v0 = i0 < len ? (int)(int8_t)buf[i0] : 0;
+                const int v1 = i1 < len ? (int)(int8_t)buf[i1] : 0;
+                const uint32_t nz0 = __ballot_sync(0xffffffffu, v0 != 0);
+                const uint32_t nz1 = __ballot_sync(0xffffffffu, v1 != 0);
+                const uint32_t ng0 = __ballot_sync(0xffffffffu, v0 < 0);
+                const uint32_t ng1 = __ballot_sync(0xffffffffu, v1 < 0);
+                if (lane == 0) {
+                    a.planes[wbase + w] = make_ulonglong2((u64)nz0 | ((u64)nz1 << 32), (u64)ng0 | ((u64)ng1 << 32));
+                    a.ckpt[wbase + w] = gs[4 * w];
+                }
+            }
+        }
+        // Mobius wheel bits for j <= mu_limit coprime to 6; groups of 32 m
+        // may straddle segments, hence atomicOr into the zeroed wheel.
+        if (low <= a.mu_limit) {
+            const i64 hi = min(end, a.mu_limit);
+            const i64 g0 = (low - 1) / 192, g1 = (hi - 1) / 192;
+            for (i64 g = g0 + warp; g <= g1; g += nwarps) {
+                const i64 m = 32 * g + lane;
+                const i64 j1 = 6 * m + 1, j5 = 6 * m + 5;
+                const int v1 = (j1 >= low && j1 <= hi) ? (int)(int8_t)buf[j1 - low] : 0;
+                const int v5 = (j5 >= low && j5 <= hi) ? (int)(int8_t)buf[j5 - low] : 0;
+                const uint32_t a1 = __ballot_sync(0xffffffffu, v1 != 0);
+                const uint32_t b1 = __ballot_sync(0xffffffffu, v1 < 0);
+                const uint32_t a5 = __ballot_sync(0xffffffffu, v5 != 0);
+                const uint32_t b5 = __ballot_sync(0xffffffffu, v5 < 0);
+                if (lane == 0) {
+                    uint32_t* wp = reinterpret_cast<uint32_t*>(a.wheel + g);
+                    if (a1) atomicOr(wp + 0, a1);
+                    if (b1) atomicOr(wp + 1, b1);
+                    if (a5) atomicOr(wp + 2, a5);
+                    if (b5) atomicOr(wp + 3, b5);
+                }
+            }
+        }
+        if (tid == 0) a.seg_sum[seg] = total;
+        __syncthreads();
+    }
+}
+
+void sieve_kernel_attrs(size_t smem, int block, int* per_sm) {
+    cudaFuncSetAttribute(sieve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    *per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, sieve_kernel, block, smem);
+}
+
+void launch_sieve(const SieveArgs& a, int grid, int block, size_t smem, cudaStream_t s) {
+    sieve_kernel<<<grid, block, smem, s>>>(a);
+}
+
+// ---------------------------------------------------------------------------
+// Segment offsets (single block) and the fix-up pass.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) seg_scan_kernel(const int32_t* in, int32_t* out, i64 n) {
+    __shared__ int32_t tile[1024];
+    __shared__ int32_t wtot[33];
+    int carry = 0;
+    for (i64 b = 0; b < n; b += 1024) {
+        const i64 i = b + threadIdx.x;
+        tile[threadIdx.x] = i < n ? in[i] : 0;
+        __syncthreads();
+        const int tot = block_excl_scan(tile, 1024, wtot);
+        if (i < n) out[i] = carry + tile[threadIdx.x];
+        carry += tot;
+        __syncthreads();
+    }
+}
+
+void launch_seg_scan(const int32_t* in, int32_t* out, i64 n, cudaStream_t s) {
+    seg_scan_kernel<<<1, 1024, 0, s>>>(in, out, n);
+}
+
+__global__ void fixup_kernel(int16_t* dM, i64 u_dense, int S, const int32_t* seg_off, int32_t* ckpt, i64 nwords,
+                             i64 dense_segs) {
+    const i64 stride = (i64)gridDim.x * blockDim.x;
+    const i64 t0 = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    const i64 n8 = (u_dense + 7) / 8;
+    for (i64 i = t0; i < n8; i += stride) {
+        const int32_t off = seg_off[(8 * i) / S];
+        if (8 * i + 8 <= u_dense) {
+            uint4* p = reinterpret_cast<uint4*>(dM) + i;
+            uint4 v = *p;
+            const uint32_t o2 = ((uint32_t)off & 0xFFFFu) * 0x10001u;
+            v.x = __vadd2(v.x, o2);
+            v.y = __vadd2(v.y, o2);
+            v.z = __vadd2(v.z, o2);
+            v.w = __vadd2(v.w, o2);
+            *p = v;
+        } else {
+            for (i64 k = 8 * i; k < u_dense; ++k) dM[k] = (int16_t)(dM[k] + off);
+        }
+    }
+    for (i64 w = t0; w < nwords; w += stride) ckpt[w] += seg_off[dense_segs + (64 * w) / S];
+}
+
+void launch_fixup(int16_t* dM, i64 u_dense, int S, const int32_t* seg_off, int32_t* ckpt, i64 nwords,
+                  i64 dense_segs, int sm_count, cudaStream_t s) {
+    const i64 work = max((u_dense + 7) / 8, nwords);
+    if (work <= 0) return;
+    const int grid = (int)std::min<i64>((work + 255) / 256, (i64)sm_count * 8);
+    fixup_kernel<<<grid, 256, 0, s>>>(dM, u_dense, S, seg_off, ckpt, nwords, dense_segs);
+}
+
+// ---------------------------------------------------------------------------
+// Planning: op counts and constant parts per evaluation slot.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int query_of_slot(const QueryDev* q, int nq, u64 s) {
+    int lo = 0, hi = nq - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (q[mid].slot_base <= s) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// counts[4*q + 0..3]: terms, evaluations, S1 lookups, S2 wheel positions
+__global__ void plan_kernel(const QueryDev* __restrict__ qs, int nq, const TableView T, u64 n_slots,
+                            u64* __restrict__ ops, u64* __restrict__ acc, i64* __restrict__ counts) {
+    const u64 stride = (u64)gridDim.x * blockDim.x;
+    for (u64 s = (u64)blockIdx.x * blockDim.x + threadIdx.x; s < n_slots; s += stride) {
+        const int qi = query_of_slot(qs, nq, s);
+        const QueryDev Q = qs[qi];
+        const u64 local = s - Q.slot_base;
+        EvalDesc d;
+        decode_eval(Q, T, (i64)(local >> 1), (int)(local & 1), d);
+        ops[s] = d.total;
+        if (d.kind != EVAL_NONE) {
+            const i64 c = d.coef * eval_constant(d, T);
+            atomicAdd(acc + 3 * qi, (u64)c);
+            unsigned long long* cq = reinterpret_cast<unsigned long long*>(counts + 4 * qi);
+            if ((local & 1) == 0) atomicAdd(cq + 0, 1ull);
+            atomicAdd(cq + 1, 1ull);
+            const u64 s1n = (u64)d.s1_cnt[0] + (u64)d.s1_cnt[1];
+            atomicAdd(cq + 2, s1n);
+            atomicAdd(cq + 3, d.total - s1n);
+        }
+    }
+}
+
+void launch_plan(const QueryDev* q, int nq, const TableView& T, u64 n_slots, u64* ops, u64* acc, i64* counts,
+                 int sm_count, cudaStream_t s) {
+    if (n_slots == 0) return;
+    const int grid = (int)std::min<u64>((n_slots + 127) / 128, (u64)sm_count * 16);
+    plan_kernel<<<grid, 128, 0, s>>>(q, nq, T, n_slots, ops, acc, counts);
+}
+
+// Direct answers for queries with X <= table u_total (get_M, :1465-1467).
+__global__ void direct_kernel(const QueryDev* qs, int nq, const TableView T, u64* acc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nq && qs[i].N == 0) acc[3 * i] = (u64)(i64)table_M(T, qs[i].X);
+}
+
+void launch_direct(const QueryDev* q, int nq, const TableView& T, u64* acc, cudaStream_t s) {
+    direct_kernel<<<(nq + 127) / 128, 128, 0, s>>>(q, nq, T, acc);
+}
+
+// ---------------------------------------------------------------------------
+// u64 exclusive scan: out[0..n] with out[n] = total (three passes).
+// ---------------------------------------------------------------------------
+constexpr int kScanBlock = 1024;
+constexpr int kScanItems = 8;
+constexpr u64 kScanTile = (u64)kScanBlock * kScanItems;
+
+__device__ u64 block_excl_scan_u64(u64 v, u64* wtot, u64* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    u64 x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const u64 t = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += t;
+    }
+    if (lane == 31) wtot[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        const u64 w = lane < nwarps ? wtot[lane] : 0;
+        u64 y = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const u64 t = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) y += t;
+        }
+        wtot[lane] = y - w;
+        if (lane == 31) wtot[32] = y;
+    }
+    __syncthreads();
+    const u64 r = wtot[warp] + x - v;
+    *total = wtot[32];
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(kScanBlock) scan_tile_sums(const u64* in, u64 n, u64* tile_sums) {
+    __shared__ u64 wtot[33];
+    const u64 base = (u64)blockIdx.x * kScanTile + (u64)threadIdx.x * kScanItems;
+    u64 s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k)
+        if (base + k < n) s += in[base + k];
+    u64 total;
+    block_excl_scan_u64(s, wtot, &total);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanBlock) scan_tile_offsets(u64* tile_sums, u64 ntiles) {
+    __shared__ u64 wtot[33];
+    u64 carry = 0;
+    for (u64 b = 0; b < ntiles; b += kScanBlock) {
+        const u64 i = b + threadIdx.x;
+        const u64 v = i < ntiles ? tile_sums[i] : 0;
+        u64 total;
+        const u64 e = block_excl_scan_u64(v, wtot, &total);
+        if (i < ntiles) tile_sums[i] = carry + e;
+        carry += total;
+    }
+    if (threadIdx.x == 0) tile_sums[ntiles] = carry;
+}
+
+__global__ void __launch_bounds__(kScanBlock) scan_tile_apply(const u64* in, u64 n, const u64* tile_off, u64* out,
+                                                              u64 ntiles) {
+    __shared__ u64 wtot[33];
+    const u64 base = (u64)blockIdx.x * kScanTile + (u64)threadIdx.x * kScanItems;
+    u64 v[kScanItems];
+    u64 s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = base + k < n ? in[base + k] : 0;
+        s += v[k];
+    }
+    u64 total;
+    u64 run = tile_off[blockIdx.x] + block_excl_scan_u64(s, wtot, &total);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) out[base + k] = run;
+        run += v[k];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = tile_off[ntiles];
+}
+
+size_t scan_u64_tmp_elems(u64 n) { return (size_t)((n + kScanTile - 1) / kScanTile) + 1; }
+
+void launch_scan_u64(const u64* in, u64* out, u64 n, u64* tmp, size_t, cudaStream_t s) {
+    const u64 ntiles = (n + kScanTile - 1) / kScanTile;
+    if (ntiles == 0) {
+        cudaMemsetAsync(out, 0, sizeof(u64), s);
+        return;
+    }
+    scan_tile_sums<<<(unsigned)ntiles, kScanBlock, 0, s>>>(in, n, tmp);
+    scan_tile_offsets<<<1, kScanBlock, 0, s>>>(tmp, ntiles);
+    scan_tile_apply<<<(unsigned)ntiles, kScanBlock, 0, s>>>(in, n, tmp, out, ntiles);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent S1 / S2 kernel over the flattened op space.
+// ---------------------------------------------------------------------------
+
+// sum of M(floor(y/n)) over n = n0 + stride*i, i in [i0, i1), lanes interleaved
+__device__ __forceinline__ i64 s1_part(const TableView& T, u64 y, i64 n0, int stride, u64 i0, u64 i1, int lane) {
+    i64 acc = 0;
+    for (u64 i = i0 + lane; i < i1; i += 32) {
+        const u64 n = (u64)n0 + (u64)stride * i;
+        const u64 q = udiv(y, n);
+        acc += table_M(T, q);
+    }
+    return acc;
+}
+
+// sum of mu(j) * piece(floor(y/j)) for j in {6m+1, 6m+5} within [jlo, jhi],
+// m = jlo/6 + i, i in [i0, i1)
+__device__ __forceinline__ u64 s2_part(const TableView& T, u64 y, const PieceCoef pc, i64 jlo, i64 jhi, u64 i0, u64 i1,
+                                       int lane) {
+    u64 acc = 0;
+    const u64 m0 = (u64)(jlo / 6);
+    for (u64 i = i0 + lane; i < i1; i += 32) {
+        const u64 m = m0 + i;
+        const uint4 w = __ldg(T.wheel + (m >> 5));
+        const uint32_t b = (uint32_t)(m & 31u);
+        const i64 j1 = (i64)(6 * m + 1), j5 = (i64)(6 * m + 5);
+        if (((w.x >> b) & 1u) && j1 >= jlo && j1 <= jhi) {
+            const i64 v = piece_eval(pc, udiv(y, (u64)j1));
+            acc += ((w.y >> b) & 1u) ? (u64)(-v) : (u64)v;
+        }
+        if (((w.z >> b) & 1u) && j5 >= jlo && j5 <= jhi) {
+            const i64 v = piece_eval(pc, udiv(y, (u64)j5));
+            acc += ((w.w >> b) & 1u) ? (u64)(-v) : (u64)v;
+        }
+    }
+    return acc;
+}
+
+__device__ __forceinline__ u64 upper_slot(const u64* prefix, u64 n_slots, u64 o) {
+    // largest s in [0, n_slots) with prefix[s] <= o
+    u64 lo = 0, hi = n_slots - 1;
+    while (lo < hi) {
+        const u64 mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= o) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(256) sums_kernel(const SumsArgs a) {
+    const int lane = threadIdx.x & 31;
+    const u64 total = a.prefix[a.n_slots];
+    int lg = a.chunk_log2;
+    if (lg <= 0) {
+        const u64 warps = (u64)gridDim.x * (blockDim.x >> 5);
+        const u64 want = total / (warps * 16) + 1;
+        lg = 64 - __clzll(want);
+        lg = max(11, min(lg, 16));
+    }
+    const u64 W = 1ull << lg;
+    int cur_q = -1;
+    u64 s1 = 0, s2 = 0;
+    for (;;) {
+        u64 chunk = 0;
+        if (lane == 0) chunk = atomicAdd(a.ticket, 1ull);
+        chunk = __shfl_sync(0xffffffffu, chunk, 0);
+        u64 o = chunk * W;
+        if (o >= total) break;
+        const u64 o_end = min(o + W, total);
+        u64 s = upper_slot(a.prefix, a.n_slots, o);
+        while (o < o_end) {
+            while (a.prefix[s + 1] <= o) ++s;
+            const u64 sbase = a.prefix[s];
+            const int qi = a.nq == 1 ? 0 : query_of_slot(a.queries, a.nq, s);
+            const QueryDev Q = a.queries[qi];
+            const u64 local = s - Q.slot_base;
+            EvalDesc d;
+            decode_eval(Q, a.T, (i64)(local >> 1), (int)(local & 1), d);
+            if (qi != cur_q) {
+                if (cur_q >= 0) {
+                    const u64 t1 = warp_sum_u64(s1), t2 = warp_sum_u64(s2);
+                    if (lane == 0) {
+                        atomicAdd(a.acc + 3 * cur_q + 1, t1);
+                        atomicAdd(a.acc + 3 * cur_q + 2, t2);
+                    }
+                }
+                s1 = s2 = 0;
+                cur_q = qi;
+            }
+            const u64 lo = o - sbase;
+            const u64 hi = min(o_end - sbase, d.total);
+            u64 segstart = 0;
+            for (int g = 0; g < d.nseg && segstart < hi; ++g) {
+                const u64 cnt = g < 2 ? (u64)d.s1_cnt[g] : (u64)d.mcnt[g - 2];
+                const u64 sb = segstart;
+                segstart += cnt;
+                const u64 a0 = max(lo, sb), a1 = min(hi, segstart);
+                if (a0 >= a1) continue;
+                if (g < 2) {
+                    const i64 part = s1_part(a.T, d.y, d.s1_n0[g], d.s1_stride[g], a0 - sb, a1 - sb, lane);
+                    const i64 sg = d.coef * d.s1_sign[g];
+                    s1 += sg > 0 ? (u64)part : (u64)(-part);
+                } else {
+                    const int p = g - 2;
+                    const u64 part = s2_part(a.T, d.y, c_piece[d.piece0 + p], d.jlo[p], d.jhi[p], a0 - sb, a1 - sb, lane);
+                    s2 += d.coef > 0 ? part : (u64)(0 - part);
+                }
+            }
+            o = sbase + hi;
+            ++s;
+        }
+    }
+    if (cur_q >= 0) {
+        const u64 t1 = warp_sum_u64(s1), t2 = warp_sum_u64(s2);
+        if (lane == 0) {
+            atomicAdd(a.acc + 3 * cur_q + 1, t1);
+            atomicAdd(a.acc + 3 * cur_q + 2, t2);
+        }
+    }
+}
+
+void sums_kernel_occupancy(int block, int* per_sm) {
+    *per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, sums_kernel, block, 0);
+}
+
+void launch_sums(const SumsArgs& a, int grid, int block, cudaStream_t s) {
+    sums_kernel<<<grid, block, 0, s>>>(a);
+}
+
+// ---------------------------------------------------------------------------
+// Table read-back and checksums (test support, reference get_M / get_mu).
+// ---------------------------------------------------------------------------
+__global__ void table_read_kernel(const TableView T, i64 first, i64 count, int32_t* M, int8_t* mu, int8_t* wmu) {
+    const i64 stride = (i64)gridDim.x * blockDim.x;
+    for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+        const i64 n = first + i;
+        const bool in = n >= 0 && n <= T.u_total;
+        const int32_t m = in ? table_M(T, (u64)n) : 0;
+        if (M) M[i] = m;
+        if (mu) mu[i] = (int8_t)((in && n >= 1 && n <= T.mu_limit) ? m - table_M(T, (u64)(n - 1)) : 0);
+        if (wmu) {
+            int v = 0;
+            if (n >= 1 && n <= T.mu_limit && (n % 2) && (n % 3)) v = wheel_mu(T.wheel, (u64)n);
+            wmu[i] = (int8_t)v;
+        }
+    }
+}
+
+void launch_table_read(const TableView& T, i64 first, i64 count, int32_t* M, int8_t* mu, int8_t* wmu, cudaStream_t s) {
+    if (count <= 0) return;
+    const int grid = (int)std::min<i64>((count + 255) / 256, 4096);
+    table_read_kernel<<<grid, 256, 0, s>>>(T, first, count, M, mu, wmu);
+}
+
+__global__ void table_sums_kernel(const TableView T, i64 nwords, u64* out) {
+    const i64 stride = (i64)gridDim.x * blockDim.x;
+    const i64 t0 = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    u64 ds = 0, dw = 0, mw = 0, nzw = 0, ngw = 0, cw = 0;
+    for (i64 n = 1 + t0; n <= T.u_dense; n += stride) {
+        const i64 v = T.dM[n - 1];
+        ds += (u64)v;
+        dw += (u64)v * (u64)(2 * n + 1);
+    }
+    for (i64 n = 1 + t0; n <= T.mu_limit; n += stride) {
+        const i64 m = (i64)table_M(T, (u64)n) - (i64)table_M(T, (u64)(n - 1));
+        mw += (u64)m * (u64)(2 * n + 1);
+    }
+    for (i64 w = t0; w < nwords; w += stride) {
+        const u64 k = (u64)(2 * w + 1);
+        const ulonglong2 p = T.planes[w];
+        nzw += p.x * k;
+        ngw += p.y * k;
+        cw += (u64)(i64)T.ckpt[w] * k;
+    }
+    ds = warp_sum_u64(ds);
+    dw = warp_sum_u64(dw);
+    mw = warp_sum_u64(mw);
+    nzw = warp_sum_u64(nzw);
+    ngw = warp_sum_u64(ngw);
+    cw = warp_sum_u64(cw);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(out + 0, ds);
+        atomicAdd(out + 1, dw);
+        atomicAdd(out + 2, mw);
+        atomicAdd(out + 3, nzw);
+        atomicAdd(out + 4, ngw);
+        atomicAdd(out + 5, cw);
+    }
+}
+
+void launch_table_sums(const TableView& T, i64 nwords, u64* out6, int sm_count, cudaStream_t s) {
+    table_sums_kernel<<<sm_count * 8, 256, 0, s>>>(T, nwords, out6);
+}
+
+// ---------------------------------------------------------------------------
+// Test support: the device quotient and S2 summand on caller-chosen inputs.
+// ---------------------------------------------------------------------------
+__global__ void debug_udiv_kernel(const u64* y, const u64* d, u64* q, i64 n) {
+    const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) q[i] = d[i] ? udiv(y[i], d[i]) : 0;
+}
+
+__global__ void debug_piece_kernel(const int32_t* piece, const u64* q, i64* out, i64 n) {
+    const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const int p = piece[i];
+        out[i] = (p >= 1 && p <= 12) ? piece_eval(c_piece[p], q[i]) : 0;
+    }
+}
+
+void launch_debug_udiv(const u64* y, const u64* d, u64* q, i64 n, cudaStream_t s) {
+    if (n > 0) debug_udiv_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(y, d, q, n);
+}
+
+void launch_debug_piece(const int32_t* piece, const u64* q, i64* out, i64 n, cudaStream_t s) {
+    if (n > 0) debug_piece_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(piece, q, out, n);
+}
+
+}  // namespace drb

@@ -1,0 +1,131 @@
+// dr_params.hpp -- parameter policy of the engine (host C++).
+//
+// DR_POLICY_REFERENCE / _DENSE / _COMPRESSED restate the reference CPU
+// engine's heuristics exactly (ecreeth/deleglise-rivat mertens_dr.hpp), so a
+// drop-in caller gets the same u, u_dense, cx and mu limit -- and therefore the
+// same intermediate S1/S2 checksums -- as the reference for the same X and
+// environment.  DR_POLICY_GPU is this engine's own default for B200.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+
+#include "../../include/dr_engine.h"
+
+namespace drb {
+
+// Exact floor square root (mertens_dr.hpp:65-74).
+inline int64_t isqrt_i64(int64_t n) {
+    if (n <= 0) return 0;
+    const uint64_t target = (uint64_t)n;
+    uint64_t s = (uint64_t)std::sqrt((double)n);
+    while ((s + 1) * (s + 1) <= target) ++s;
+    while (s * s > target) --s;
+    return (int64_t)s;
+}
+
+// choose_cx (mertens_dr.hpp:914-923); MERTENS_CX in (0.1, 5.0) overrides.
+inline double ref_choose_cx(int64_t X) {
+    if (const char* e = std::getenv("MERTENS_CX")) {
+        const double v = std::atof(e);
+        if (v > 0.1 && v < 5.0) return v;
+    }
+    if (X >= 1000000000000000LL) return 1.35;
+    if (X >= 10000000000000LL) return 1.15;
+    if (X >= 100000000000LL) return 0.95;
+    return 0.70;
+}
+
+// choose_sieve_limit (mertens_dr.hpp:931-962); MERTENS_FX, MERTENS_U_CAP.
+inline int64_t ref_choose_sieve_limit(int64_t X) {
+    if (X <= 50000000LL) return X;
+    const double loglogX = std::log(std::max(2.0, std::log((double)X)));
+    double fx = 0.32;
+    if (const char* e = std::getenv("MERTENS_FX")) {
+        const double v = std::atof(e);
+        if (v >= 0.1 && v <= 3.0) fx = v;
+    }
+    int64_t u = (int64_t)(fx * std::pow((double)X / loglogX, 2.0 / 3.0));
+    const int64_t S = isqrt_i64(X);
+    if (u < 3 * S) u = 3 * S;
+    int64_t cap = 1500000000LL;
+    if (const char* e = std::getenv("MERTENS_U_CAP")) {
+        const int64_t v = (int64_t)std::atoll(e);
+        if (v >= 100000000LL && v <= 4000000000LL) cap = v;
+    }
+    return std::min(u, cap);
+}
+
+// choose_compressed_limit (mertens_dr.hpp:1401-1419); MERTENS_CHMT_U_CAP.
+inline int64_t ref_choose_compressed_limit(int64_t X) {
+    if (X < 50000000LL) return X;
+    const double loglogX = std::log(std::max(2.0, std::log((double)X)));
+    double fx = 0.95;
+    if (X >= 1000000000000000LL) fx = 1.25;
+    if (X >= 10000000000000000LL) fx = 1.50;
+    int64_t u = (int64_t)(fx * std::pow((double)X / loglogX, 2.0 / 3.0));
+    const int64_t S = isqrt_i64(X);
+    if (u < 3 * S) u = 3 * S;
+    u = ((u + 255) / 256) * 256;
+    int64_t cap = 8000000000LL;
+    if (const char* e = std::getenv("MERTENS_CHMT_U_CAP")) {
+        const int64_t v = (int64_t)std::atoll(e);
+        if (v >= 100000000LL && v <= 10000000000LL) cap = v;
+    }
+    const int64_t endpoints = (int64_t)(ref_choose_cx(X) * std::sqrt((double)X)) + 1000;
+    cap = std::max(cap, std::max(S + 1000, endpoints));
+    return std::min(u, cap);
+}
+
+// Strategy switch (mertens_dr.hpp:1027-1029, 1421-1435; x86-64 default rule).
+inline bool ref_use_compressed(int64_t X) {
+    bool on;
+    if (const char* e = std::getenv("MERTENS_USE_CHMT")) {
+        on = (e[0] == '1' || e[0] == 'y' || e[0] == 'Y' || e[0] == 't' || e[0] == 'T');
+    } else {
+        on = X >= 100000000000LL && !std::getenv("MERTENS_FX") && !std::getenv("MERTENS_U_CAP");
+    }
+    return X >= 100000000000LL && on;
+}
+
+inline void params_clear(dr_params* p) {
+    p->u_total = p->u_dense = p->mu_limit = 0;
+    p->cx = 0.0;
+    p->segment_log2 = p->block_threads = p->chunk_log2 = p->reserved = 0;
+}
+
+// Dense path parameters (mertens_dr.hpp:1033-1041 with SieveTable's clamp :396).
+inline void ref_dense_params(int64_t X, dr_params* p) {
+    params_clear(p);
+    const double cx = ref_choose_cx(X);
+    const int64_t u = ref_choose_sieve_limit(X);
+    const int64_t N = X / u;
+    const int64_t A_max = (int64_t)(cx * std::sqrt((double)X)) + 1000;
+    const int64_t mu_limit = std::max(A_max, N + 1000);
+    p->u_total = u;
+    p->u_dense = u;
+    p->cx = cx;
+    p->mu_limit = (X <= u) ? u : std::min(mu_limit, u);
+}
+
+// Streamed path parameters (mertens_dr.hpp:1451-1463 with the table clamps :691, :701).
+inline void ref_compressed_params(int64_t X, dr_params* p) {
+    params_clear(p);
+    const double cx = ref_choose_cx(X);
+    const int64_t u_total = ref_choose_compressed_limit(X);
+    int64_t endpoint = (int64_t)(cx * std::sqrt((double)X)) + 1000;
+    endpoint = (endpoint + 255) & ~255LL;
+    const int64_t dense_target = std::min<int64_t>(128000000LL, ((u_total / 4 + 255) & ~255LL));
+    const int64_t u_dense = std::min(u_total, std::max(dense_target, endpoint));
+    const int64_t N = X / u_total;
+    const int64_t A_max = (int64_t)(cx * std::sqrt((double)X)) + 1000;
+    const int64_t mu_limit = std::max(A_max, N + 1000);
+    p->u_total = u_total;
+    p->u_dense = u_dense;
+    p->cx = cx;
+    p->mu_limit = std::min(u_total, mu_limit);
+}
+
+}  // namespace drb

@@ -1,0 +1,132 @@
+/*
+ * dr_engine.h -- C ABI of the B200 Deleglise-Rivat Mertens engine (libdrb200.so).
+ *
+ * Everything below is plain C: integers, doubles, pointers and sizes.  No
+ * exceptions cross this boundary; every entry point returns an int status
+ * (DR_OK = 0, negative on error) and dr_last_error() describes the last
+ * failure on the calling thread.  Device memory is owned by an opaque
+ * dr_ctx (one CUDA stream per context).  A context is not thread-safe;
+ * separate contexts are.
+ *
+ * Reference interfaces replaced (ecreeth/deleglise-rivat):
+ *   dr_mertens()            <- DelégliseRivatEngine::compute_mertens(int64 X, int threads)
+ *                              mertens_dr.hpp:968, and ::compute_compressed(int64, int)
+ *                              mertens_dr.hpp:1442 (policy DR_POLICY_REFERENCE picks the
+ *                              same dense/streamed parameters); also
+ *                              CudaDelégliseRivatEngine::compute_mertens(int64, int,
+ *                              TimingStats*) mertens_cuda.cuh:441 (timings in dr_stats).
+ *   dr_default_params()     <- choose_cx :914, choose_sieve_limit :931,
+ *                              choose_compressed_limit :1401, dense target and mu limit
+ *                              :1033-1038, :1451-1461, use_compressed_default :1421,
+ *                              use_chmt_env :1430 (MERTENS_* environment overrides).
+ *   dr_table_build() / dr_table_read() / dr_table_checksums()
+ *                           <- CompressedMertensTable(u_total, u_dense, threads, max_mu)
+ *                              mertens_dr.hpp:689, get_M :707, get_mu :714 and the raw
+ *                              members dense_M/mu/chunks/checkpoints :681-687 (SieveTable
+ *                              :376-457 when u_dense == u_total).
+ *   dr_mertens_batch()      <- no counterpart (the reference evaluates one X per call);
+ *                              it is the batched mode of compute_mertens.
+ */
+#ifndef DR_ENGINE_H
+#define DR_ENGINE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DR_OK 0
+#define DR_ERR_ARG -1     /* invalid argument                              */
+#define DR_ERR_PARAMS -2  /* parameters fail the endpoint-coverage check   */
+#define DR_ERR_NOMEM -3   /* device or host allocation failed / over budget */
+#define DR_ERR_CUDA -4    /* CUDA runtime error                            */
+#define DR_ERR_DEVICE -5  /* device-side check failed (error flag set)     */
+
+/* Parameter policies for dr_default_params(). */
+#define DR_POLICY_REFERENCE 0 /* exactly the reference CPU engine's choice  */
+#define DR_POLICY_DENSE 1     /* reference dense path (MERTENS_USE_CHMT=0)  */
+#define DR_POLICY_COMPRESSED 2 /* reference streamed path (compute_compressed) */
+#define DR_POLICY_GPU 3       /* B200 defaults: larger u, compressed tier   */
+
+typedef struct dr_ctx dr_ctx;
+
+typedef struct {
+    int64_t u_total;     /* sieve / table limit u                               */
+    int64_t u_dense;     /* dense int16 prefix covers 0..u_dense (<= u_total)   */
+    double cx;           /* S1/S2 split, A = floor(cx*sqrt(y)) (parameter only) */
+    int64_t mu_limit;    /* Mobius values kept for 1..mu_limit                  */
+    int32_t segment_log2;/* sieve segment = 2^segment_log2 values (0: default)  */
+    int32_t block_threads;/* threads per sieve CTA (0: default)                 */
+    int32_t chunk_log2;  /* S1/S2 work item = 2^chunk_log2 ops (0: default)    */
+    int32_t reserved;
+} dr_params;
+
+typedef struct {
+    int64_t M;               /* M(X)                                           */
+    uint64_t C, S1, S2;      /* checksums: M = C - S1 - S2 (mod 2^64)           */
+    int64_t terms, evals;    /* outer terms, single/comb2 evaluations           */
+    uint64_t s1_ops, s2_ops; /* S1 lookups, S2 wheel positions (2 j each)       */
+    double table_ms;         /* device time: sieve + prefix + compressed tier   */
+    double plan_ms;          /* device time: term list, op counts, scan         */
+    double sums_ms;          /* device time: persistent S1/S2 kernel            */
+    double total_ms;         /* host wall time of the call                      */
+    double h2d_ms, d2h_ms;   /* copies (batched inputs / results)              */
+    int32_t sieve_launches, sums_launches, kernel_launches;
+    int32_t reserved;
+} dr_stats;
+
+typedef struct {
+    uint64_t dense_sum, dense_wsum, mu_wsum, nz_wsum, neg_wsum, ckpt_wsum;
+} dr_table_sums;
+
+/* Context -------------------------------------------------------------- */
+int dr_ctx_create(int device, void *cuda_stream /* NULL: own stream */, dr_ctx **out);
+int dr_ctx_destroy(dr_ctx *ctx);
+const char *dr_last_error(void);
+/* Cap on device bytes the context may hold (0: 90% of free memory at create). */
+int dr_ctx_set_hbm_budget(dr_ctx *ctx, uint64_t bytes);
+int dr_device_info(int device, int *sm_count, uint64_t *hbm_bytes);
+
+/* Parameters ------------------------------------------------------------- */
+int dr_default_params(int64_t X, int policy, dr_params *out);
+/* Endpoint-coverage and budget check (0 = usable). */
+int dr_check_params(int64_t X, const dr_params *p, uint64_t hbm_budget);
+/* Device bytes a table with these limits needs. */
+uint64_t dr_table_bytes(int64_t u_total, int64_t u_dense, int64_t mu_limit);
+
+/* Single query (reference: compute_mertens / compute_compressed) ------------- */
+int dr_mertens(dr_ctx *ctx, int64_t X, const dr_params *p /* NULL: reference policy */,
+               int64_t *out, dr_stats *stats /* nullable */);
+
+/* Batched queries: one shared table, one persistent launch for all S1/S2 work.
+ * p: one params struct per query (NULL: reference policy per X) -- the table is
+ * built to cover the largest u_total/u_dense/mu_limit among them. */
+int dr_mertens_batch(dr_ctx *ctx, const int64_t *X, int64_t count, const dr_params *p,
+                     int64_t *out, dr_stats *stats);
+/* Per-query checksums of the last batch (count x {C, S1, S2}). */
+int dr_batch_checksums(dr_ctx *ctx, uint64_t *out3, int64_t count);
+
+/* Tables (reference: CompressedMertensTable / SieveTable) -------------------- */
+int dr_table_build(dr_ctx *ctx, int64_t u_total, int64_t u_dense, int64_t mu_limit,
+                   const dr_params *tuning /* nullable: segment / block shape */,
+                   dr_stats *stats);
+/* M(n) and mu(n) for n in [first, first+count), any pointer may be NULL. */
+int dr_table_read(dr_ctx *ctx, int64_t first, int64_t count, int32_t *M, int8_t *mu);
+int dr_table_checksums(dr_ctx *ctx, dr_table_sums *out);
+/* Mobius values as held in the mod-6 wheel that S2 and the term list read
+ * (0 for n sharing a factor with 6 or n > mu_limit); test support. */
+int dr_table_read_wheel(dr_ctx *ctx, int64_t first, int64_t count, int8_t *mu);
+
+/* Test support: the device's exact quotient floor(y[i]/d[i]) and S2 summand
+ * piece[i](q[i]) (pieces 1..8 combined, 9..12 single) on host arrays.  The
+ * reference has no counterpart (its quotients are fast_div, mertens_dr.hpp:80,
+ * and its summands Piece1..SinglePiece4, :470-482). */
+int dr_debug_udiv(dr_ctx *ctx, const uint64_t *y, const uint64_t *d, int64_t n, uint64_t *q);
+int dr_debug_piece(dr_ctx *ctx, const int32_t *piece, const uint64_t *q, int64_t n, int64_t *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DR_ENGINE_H */

@@ -1,0 +1,80 @@
+"""GPU: the device's exact quotient and S2 summands.
+
+Every S1 lookup and S2 term of the engine goes through these two routines, so
+they are checked exhaustively on edge classes: y near 2^53 (where the
+reference switches from double to integer division, mertens_dr.hpp:80-86),
+2^63 - 1, 10^18, divisors near sqrt(y), y/u, 2^31, 2^32 and above.
+"""
+import random
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _edge_pairs():
+    ys = [0, 1, 2, 3, 11, 12, 13, 2**31 - 1, 2**31, 2**32 - 1, 2**32, 2**32 + 1, 2**40 + 7,
+          2**53 - 1, 2**53, 2**53 + 1, 2**53 + 2, 10**16, 10**16 + 1, 10**17, 10**18 - 1, 10**18, 10**18 + 1,
+          2**62, 2**63 - 1, 2**63, 2**64 - 1]
+    pairs = []
+    for y in ys:
+        r = int(y**0.5)
+        ds = [1, 2, 3, 5, 6, 7, 12, 97, 65535, 65536, 2**31 - 1, 2**31, 2**32 - 1, 2**32, 2**32 + 1, 2**40 + 3,
+              max(1, r - 1), max(1, r), r + 1, max(1, y // 8000000000), y // 8000000000 + 1,
+              max(1, y // 400000000000), max(1, y) if y else 1]
+        for d in ds:
+            if d >= 1:
+                pairs.append((y, d))
+    return pairs
+
+
+def test_udiv_edges(engine):
+    pairs = _edge_pairs()
+    ys, ds = zip(*pairs)
+    q = engine.debug_udiv(ys, ds)
+    for (y, d), got in zip(pairs, q):
+        assert got == y // d, (y, d, got)
+
+
+def test_udiv_random(engine):
+    rng = random.Random(20261203)
+    ys, ds = [], []
+    for _ in range(200000):
+        bits = rng.choice([20, 32, 40, 53, 54, 60, 63, 64])
+        y = rng.getrandbits(bits)
+        dbits = rng.choice([1, 8, 16, 24, 31, 32, 33, 40])
+        d = max(1, rng.getrandbits(dbits))
+        ys.append(y)
+        ds.append(d)
+    q = engine.debug_udiv(ys, ds)
+    bad = [(y, d, g) for y, d, g in zip(ys, ds, q) if g != y // d]
+    assert not bad, bad[:5]
+
+
+def test_udiv_s1_shapes(engine):
+    # consecutive n near sqrt(y)/cx and near y/u for y = X/k at X = 10^16, 10^18
+    ys, ds = [], []
+    for X in (10**16, 10**18, 2**63 - 1):
+        for k in (1, 5, 7, 11, 1001, 99991):
+            y = X // k
+            r = int((y / 1.35) ** 0.5)
+            for n in list(range(r - 300, r + 300)) + list(range(y // 8000000000 + 1, y // 8000000000 + 300)):
+                if n >= 1:
+                    ys.append(y)
+                    ds.append(n)
+    q = engine.debug_udiv(ys, ds)
+    assert all(g == y // d for y, d, g in zip(ys, ds, q))
+
+
+def test_pieces_match_oracle(engine, oracle):
+    rng = random.Random(5)
+    qs = list(range(0, 300)) + [rng.getrandbits(b) for b in (20, 40, 53, 60, 62) for _ in range(200)]
+    qs += [2**53 - 1, 2**53, 2**53 + 1, 10**18, 2**63 - 1]
+    pieces, vals = [], []
+    for p in range(1, 13):
+        for q in qs:
+            pieces.append(p)
+            vals.append(q)
+    got = engine.debug_piece(pieces, vals)
+    for p, q, g in zip(pieces, vals, got):
+        assert g == oracle.piece(p, q), (p, q, g)

@@ -1,0 +1,42 @@
+"""GPU: batched queries in one table build and one persistent S1/S2 launch.
+
+The batch of 256 X = round(10^U), U ~ U(9, 14), seed 20261203, is checked
+bit-exact against the reference's compute_mertens (tests/golden/batch256.json).
+Per-query checksums of a batch equal those of single calls with the same
+parameters.
+"""
+import random
+
+import pytest
+
+import dr_b200
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def test_batch256_golden(engine):
+    g = load_golden("batch256.json")
+    got, st = engine.mertens_batch(g["X"])
+    assert got == g["M"]
+    assert st.sums_launches == 1 and st.sieve_launches == 1
+
+
+def test_batch_checksums_equal_single(engine):
+    rng = random.Random(3)
+    xs = [int(10 ** rng.uniform(9, 12)) for _ in range(12)] + [10**12, 7, 10**5]
+    ps = [dr_b200.default_params(x, dr_b200.POLICY_COMPRESSED) for x in xs]
+    got, _ = engine.mertens_batch(xs, ps)
+    sums = engine.batch_checksums(len(xs))
+    for x, p, m, s in zip(xs, ps, got, sums):
+        r = engine.mertens(x, p)
+        assert r.M == m
+        if x > p.u_total:
+            assert (r.stats.C, r.stats.S1, r.stats.S2) == s, x
+
+
+def test_batch_mixed_sizes(engine, oracle):
+    xs = [1, 2, 3, 10, 99975680, 10**6, 10**11, 123456789012, 5, 10**12, 0]
+    got, _ = engine.mertens_batch(xs)
+    for x, m in zip(xs, got):
+        assert m == (oracle.mertens(x) if x > 0 else 0), x

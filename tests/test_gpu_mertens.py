@@ -1,0 +1,92 @@
+"""GPU: M(X) and the C/S1/S2 checksums vs the reference and the oracle.
+
+* known answers 1 .. 10^17 (test_dr.cpp:26-47, test_cuda.cu:38-60, README.md:188),
+* the reference's own C/S1/S2 checksums at its default parameters, dense and
+  streamed, up to 10^16 (tests/golden/checksums.json from oracle/_ref),
+* random X with randomised parameters against the oracle (any valid
+  parameters give the same M(X); the checksums must match at equal ones),
+* boundary inputs: tiny X, X = u, X = u + 1, the dense/compressed quotient
+  boundary X = 99,975,680 (test_sieve.cpp:206-209).
+"""
+import random
+
+import pytest
+
+import dr_b200
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _p(c):
+    return dr_b200.Params(u_total=c["u_total"], u_dense=c["u_dense"], cx=c["cx"], mu_limit=c["mu_limit"])
+
+
+def test_known_answers(engine):
+    for c in load_golden("kat.json")["cases"]:
+        assert engine.compute_mertens(c["X"]) == c["M"], c
+
+
+def test_known_answers_compressed_policy(engine):
+    for c in load_golden("kat.json")["cases"]:
+        if c["X"] >= 10**5:
+            assert engine.compute_compressed(c["X"]) == c["M"], c
+
+
+def test_reference_checksums(engine):
+    for c in load_golden("checksums.json")["cases"]:
+        r = engine.mertens(c["X"], _p(c))
+        s = r.stats
+        assert (r.M, s.C, s.S1, s.S2, s.terms) == (c["M"], c["C"], c["S1"], c["S2"], c["terms"]), c
+
+
+def test_random_params_vs_oracle(engine, oracle):
+    rng = random.Random(20261203)
+    for _ in range(40):
+        X = int(10 ** rng.uniform(6, 11.5))
+        p = dr_b200.default_params(X, dr_b200.POLICY_COMPRESSED)
+        cx = rng.uniform(0.3, 3.0)
+        A = int(cx * X**0.5)
+        u = max(p.u_total, A + 2000, int(X**0.5) * 3)
+        u = rng.randint(max(A + 2, 3 * int(X**0.5)), max(A + 2, 3 * int(X**0.5)) * 4)
+        ud = rng.randint(0, u)
+        ml = rng.randint(min(u, max(A, X // u) + 1), u)
+        q = dr_b200.Params(u_total=u, u_dense=ud, cx=cx, mu_limit=ml, segment_log2=rng.choice([12, 14, 16, 17]))
+        r = engine.mertens(X, q)
+        o = oracle.run(X, u, ud, cx, ml)
+        assert (r.M, r.stats.C, r.stats.S1, r.stats.S2) == (o["M"], o["C"], o["S1"], o["S2"]), (X, q)
+
+
+def test_small_and_boundary_inputs(engine, oracle):
+    for X in list(range(0, 200)) + [1000, 10**5, 10**5 + 1, 5 * 10**7, 5 * 10**7 + 1, 99975680]:
+        want = oracle.mertens(X) if X > 0 else 0
+        assert engine.compute_mertens(X) == want, X
+        if X > 100000:
+            assert engine.compute_compressed(X) == want, X
+    # X at and just above the table limit
+    for X in (10**9, 10**10):
+        p = dr_b200.default_params(X, dr_b200.POLICY_COMPRESSED)
+        for u in (p.u_total, X - 1, X, X + 1):
+            u = min(u, X + 1)
+            q = dr_b200.Params(u_total=u, u_dense=min(u, p.u_dense), cx=p.cx, mu_limit=min(u, p.mu_limit))
+            if dr_b200.check_params(X, q) != 0:
+                continue
+            assert engine.mertens(X, q).M == oracle.mertens(X)
+
+
+def test_dense_config_1e12(engine):
+    # config: plain dense M(10^12), MERTENS_USE_CHMT=0 parameters
+    p = dr_b200.default_params(10**12, dr_b200.POLICY_DENSE)
+    assert p.u_total == p.u_dense == 14381928
+    r = engine.mertens(10**12, p)
+    assert r.M == 62366
+
+
+def test_bad_params_raise(engine):
+    p = dr_b200.default_params(10**12)
+    bad = dr_b200.Params(**{**p.as_dict(), "mu_limit": 5})
+    with pytest.raises(dr_b200.DRError) as ei:
+        engine.mertens(10**12, bad)
+    assert ei.value.code == dr_b200.DR_ERR_PARAMS
+    # the context stays usable after a rejected call
+    assert engine.compute_mertens(10**9) == -222
