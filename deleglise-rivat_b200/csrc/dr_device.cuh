@@ -62,7 +62,8 @@ __device__ __forceinline__ u64 udiv(u64 y, u64 d) {
 // B/6 A/6 B/3 A/3 B/2 A/2 B A); single pieces 9..12 are f_A(q) (cut at A/6
 // A/3 A/2 A).  Each is additive over q = 12k + r:
 //   piece(q) = piece(12) * k + piece(r),
-// so the device evaluates a*k + T[r] with T packed as 4-bit nibbles (+8).
+// so the device evaluates a*k + T[r] with T packed as 5-bit fields (+16);
+// T[r] ranges over [-1, 11] (piece(q) = q has T[r] = r).
 // ---------------------------------------------------------------------------
 __host__ __device__ constexpr i64 piece_formula(int piece, i64 q) {
     const i64 h = q / 2, t = q / 3, f = q / 4, s = q / 6, d = q / 12;
@@ -85,19 +86,19 @@ __host__ __device__ constexpr i64 piece_formula(int piece, i64 q) {
 
 struct PieceCoef {
     i64 a;       // piece(12)
-    u64 packed;  // nibble r holds piece(r) + 8, r = 0..11
+    u64 packed;  // bits 5r..5r+4 hold piece(r) + 16, r = 0..11
 };
 
 __host__ __device__ constexpr PieceCoef make_piece_coef(int piece) {
     PieceCoef c{piece_formula(piece, 12), 0};
-    for (int r = 0; r < 12; ++r) c.packed |= (u64)(piece_formula(piece, r) + 8) << (4 * r);
+    for (int r = 0; r < 12; ++r) c.packed |= (u64)(piece_formula(piece, r) + 16) << (5 * r);
     return c;
 }
 
 __device__ __forceinline__ i64 piece_eval(const PieceCoef& c, u64 q) {
     const u64 k = q / 12u;
     const uint32_t r = (uint32_t)(q - k * 12u);
-    const int t = (int)((c.packed >> (4 * r)) & 15u) - 8;
+    const int t = (int)((c.packed >> (5 * r)) & 31u) - 16;
     return c.a * (i64)k + t;
 }
 

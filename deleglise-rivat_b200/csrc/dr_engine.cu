@@ -328,8 +328,8 @@ int run_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, int
     if ((rc = ensure(c, c->ops, (size_t)std::max<u64>(slots, 1) * 8))) return rc;
     if ((rc = ensure(c, c->prefix, (size_t)(slots + 1) * 8))) return rc;
     if ((rc = ensure(c, c->scan_tmp, scan_u64_tmp_elems(slots) * 8))) return rc;
-    if ((rc = ensure(c, c->ticket, 8))) return rc;
-    const size_t need_pinned = (size_t)nq * 7;
+    if ((rc = ensure(c, c->ticket, 16))) return rc;
+    const size_t need_pinned = (size_t)nq * 7 + 2;
     if (c->pinned_cap < need_pinned) {
         if (c->pinned) cudaFreeHost(c->pinned);
         c->pinned = nullptr;
@@ -342,7 +342,7 @@ int run_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, int
     CU(cudaMemcpyAsync(c->queries.p, qs.data(), (size_t)nq * sizeof(QueryDev), cudaMemcpyHostToDevice, c->stream));
     CU(cudaMemsetAsync(c->acc.p, 0, (size_t)nq * 3 * 8, c->stream));
     CU(cudaMemsetAsync(c->counts.p, 0, (size_t)nq * 4 * 8, c->stream));
-    CU(cudaMemsetAsync(c->ticket.p, 0, 8, c->stream));
+    CU(cudaMemsetAsync(c->ticket.p, 0, 16, c->stream));
     launch_direct((const QueryDev*)c->queries.p, qn, T, (u64*)c->acc.p, c->stream);
     int launches = 1;
     if (slots > 0) {
@@ -376,14 +376,20 @@ int run_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, int
     CU(cudaMemcpyAsync(c->pinned, c->acc.p, (size_t)nq * 3 * 8, cudaMemcpyDeviceToHost, c->stream));
     CU(cudaMemcpyAsync(c->pinned + (size_t)nq * 3, c->counts.p, (size_t)nq * 4 * 8, cudaMemcpyDeviceToHost,
                        c->stream));
+    CU(cudaMemcpyAsync(c->pinned + (size_t)nq * 7, c->ticket.p, 16, cudaMemcpyDeviceToHost, c->stream));
     CU(cudaEventRecord(c->ev[5], c->stream));
     CU(cudaStreamSynchronize(c->stream));
     CU(cudaGetLastError());
-    c->last_sums.assign(c->pinned, c->pinned + (size_t)nq * 3);
+    if (c->pinned[(size_t)nq * 7 + 1])
+        return fail(DR_ERR_DEVICE, "sums kernel: op count of an evaluation disagreed with its plan");
     for (int64_t i = 0; i < nq; ++i) {
-        const uint64_t* a = c->pinned + 3 * i;
+        uint64_t* a = c->pinned + 3 * i;
         out[i] = X[i] < 1 ? 0 : (int64_t)(a[0] - a[1] - a[2]);
+        // X <= u is answered from the table alone: no terms, so no checksums
+        // (the reference returns get_M(X) there, mertens_dr.hpp:1465-1467)
+        if (qs[(size_t)i].N == 0) a[0] = a[1] = a[2] = 0;
     }
+    c->last_sums.assign(c->pinned, c->pinned + (size_t)nq * 3);
     if (st) {
         float ms = 0;
         cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);

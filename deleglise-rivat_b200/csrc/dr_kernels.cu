@@ -554,6 +554,12 @@ __global__ void __launch_bounds__(256) sums_kernel(const SumsArgs a) {
             }
             const u64 lo = o - sbase;
             const u64 hi = min(o_end - sbase, d.total);
+            if (hi <= lo) {
+                // planning and decoding disagree on this slot's op count: flag
+                // it and abandon the chunk instead of spinning without progress
+                if (lane == 0) atomicOr(a.ticket + 1, 1ull);
+                break;
+            }
             u64 segstart = 0;
             for (int g = 0; g < d.nseg && segstart < hi; ++g) {
                 const u64 cnt = g < 2 ? (u64)d.s1_cnt[g] : (u64)d.mcnt[g - 2];

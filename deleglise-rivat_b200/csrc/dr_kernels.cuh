@@ -34,7 +34,7 @@ struct SumsArgs {
     TableView T;
     u64 n_slots;
     const u64* prefix;  // [n_slots + 1] exclusive op prefix
-    u64* ticket;        // work-queue counter, zeroed before launch
+    u64* ticket;        // [0]: work-queue counter, [1]: error flag; zeroed before launch
     u64* acc;           // [3 * nq]: C, S1, S2
     int chunk_log2;     // 0: chosen on the device from the total
 };
