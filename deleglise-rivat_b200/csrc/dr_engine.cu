@@ -26,15 +26,13 @@ using namespace drb;
 
 namespace {
 
-thread_local std::string g_err = "";
+thread_local char g_err[512] = "";
 
 int fail(int code, const char* fmt, ...) {
-    char buf[512];
     va_list ap;
     va_start(ap, fmt);
-    vsnprintf(buf, sizeof(buf), fmt, ap);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
     va_end(ap);
-    g_err = buf;
     return code;
 }
 
@@ -59,6 +57,8 @@ double now_ms() {
 }
 
 }  // namespace
+
+int drb::record_error(int code, const char* msg) { return fail(code, "%s", msg); }
 
 struct dr_ctx {
     int device = 0;
@@ -423,7 +423,7 @@ int run_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, int
 // ===========================================================================
 extern "C" {
 
-const char* dr_last_error(void) { return g_err.c_str(); }
+const char* dr_last_error(void) { return g_err; }
 
 int dr_device_info(int device, int* sm_count, uint64_t* hbm_bytes) {
     cudaDeviceProp prop;

@@ -54,6 +54,8 @@ void launch_table_read(const TableView& T, i64 first, i64 count, int32_t* M, int
                        cudaStream_t s);
 void launch_table_sums(const TableView& T, i64 nwords, u64* out6, int sm_count, cudaStream_t s);
 void init_piece_constants();
+// Record a message for dr_last_error() (fixed thread-local buffer) and return code.
+int record_error(int code, const char* msg);
 // Opt the sieve kernel into `smem` bytes of dynamic shared memory and report
 // how many CTAs of `block` threads fit on one SM.
 void sieve_kernel_attrs(size_t smem, int block, int* per_sm);

@@ -1,0 +1,207 @@
+// dr_noalloc.cu -- a table build that allocates no memory at all.
+//
+// Who needs it: code that owns device memory through its own allocator and is
+// not allowed to call cudaMalloc/cudaFree behind that allocator's back -- a
+// framework's caching allocator, a memory pool reserved up front, a service
+// that must not allocate once it is serving.  Such a caller hands in the table
+// buffers it allocated itself; everything else the build needs (per-segment
+// Mobius sums and their offsets, the sieving primes, the periodic stencil)
+// lives in one file-scope __device__ array of fixed size.
+//
+// It runs the same kernels as dr_table_build() (sieve_kernel, seg_scan_kernel,
+// fixup_kernel) and produces the same table, bit for bit.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <mutex>
+
+#include "../../include/dr_engine.h"
+#include "dr_kernels.cuh"
+
+using namespace drb;
+
+namespace {
+
+constexpr int kNoAllocSegLog2 = 17;
+constexpr int kNoAllocSeg = 1 << kNoAllocSegLog2;          // values per sieve segment
+constexpr int64_t kNoAllocMaxSegs = DR_NOALLOC_MAX_U / kNoAllocSeg + 2;  // dense + compressed runs
+constexpr int kNoAllocMaxRoot = 92681;                       // isqrt(DR_NOALLOC_MAX_U)
+constexpr int kNoAllocMaxPrimes = 9216;                      // pi(92681) = 8952
+constexpr int kMaxDevices = 64;
+
+// scratch layout, in 32-bit words
+constexpr size_t kOffStencil = 0;
+constexpr size_t kOffSegSum = kOffStencil + (size_t)4 * kStencilWords;
+constexpr size_t kOffSegOff = kOffSegSum + (size_t)kNoAllocMaxSegs;
+constexpr size_t kOffPrimes = kOffSegOff + (size_t)kNoAllocMaxSegs;
+constexpr size_t kScratchWords = kOffPrimes + (size_t)kNoAllocMaxPrimes;  // 616,624 bytes
+
+// The scratch.  In host code this name is only a host-side stand-in for the
+// symbol, never a device address: the device address comes from
+// cudaGetSymbolAddress() below, once per device.
+static __device__ __align__(256) uint32_t g_table_scratch[kScratchWords];
+
+// Host-side constant inputs, filled once per process (static storage, no heap).
+uint32_t g_host_primes[kNoAllocMaxPrimes];
+int g_host_prime_count = 0;
+uint32_t g_host_stencil[4 * kStencilWords];
+std::once_flag g_host_once;
+
+void fill_host_constants() {
+    static uint8_t composite[kNoAllocMaxRoot + 1];
+    for (int64_t p = 2; p <= kNoAllocMaxRoot; ++p) {
+        if (composite[p]) continue;
+        g_host_primes[g_host_prime_count++] = (uint32_t)p;
+        for (int64_t m = p * p; m <= kNoAllocMaxRoot; m += p) composite[m] = 1;
+    }
+    // periodic stencil, 4 copies shifted by 0..3 bytes; byte i describes n = i + 1
+    auto stencil_byte = [](int i) -> uint32_t {
+        const int n = (i % kStencilPeriod) + 1;
+        uint32_t a = 0;
+        const int small[5] = {2, 3, 5, 7, 11};
+        for (int p : small)
+            if (n % p == 0) a += (uint32_t)((32 - __builtin_clz((unsigned)(p - 1))) | 1);
+        if (n % 4 == 0 || n % 9 == 0) a |= 0x80u;
+        return a;
+    };
+    for (int s = 0; s < 4; ++s)
+        for (int w = 0; w < kStencilWords; ++w) {
+            uint32_t v = 0;
+            for (int b = 0; b < 4; ++b) v |= stencil_byte(4 * w + s + b) << (8 * b);
+            g_host_stencil[(size_t)s * kStencilWords + (size_t)w] = v;
+        }
+}
+
+struct DeviceSetup {
+    std::once_flag once;
+    int status = DR_OK;
+    uint32_t* scratch = nullptr;  // device address of g_table_scratch on this device
+    int sieve_per_sm = 1;
+    int sm_count = 1;
+};
+DeviceSetup g_dev[kMaxDevices];
+
+int noalloc_fail(int code, const char* msg, cudaError_t e = cudaSuccess) {
+    char buf[256];
+    if (e != cudaSuccess) snprintf(buf, sizeof(buf), "dr_table_build_noalloc: %s: %s", msg, cudaGetErrorString(e));
+    else snprintf(buf, sizeof(buf), "dr_table_build_noalloc: %s", msg);
+    return record_error(code, buf);
+}
+
+// Once per device, with that device current: resolve the scratch's device
+// address and fill its constant parts (stencil, primes).
+void setup_device(int device, DeviceSetup& d) {
+    std::call_once(g_host_once, fill_host_constants);
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_table_scratch);
+    if (e != cudaSuccess || !ptr) {
+        d.status = noalloc_fail(DR_ERR_CUDA, "cudaGetSymbolAddress(g_table_scratch) failed", e);
+        return;
+    }
+    d.scratch = (uint32_t*)ptr;
+    e = cudaMemcpy(d.scratch + kOffStencil, g_host_stencil, sizeof(g_host_stencil), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(d.scratch + kOffPrimes, g_host_primes, sizeof(uint32_t) * (size_t)g_host_prime_count,
+                       cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        d.status = noalloc_fail(DR_ERR_CUDA, "filling the table scratch failed", e);
+        return;
+    }
+    e = cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) {
+        d.status = noalloc_fail(DR_ERR_CUDA, "cudaDeviceGetAttribute failed", e);
+        return;
+    }
+    sieve_kernel_attrs(sieve_smem_bytes(kNoAllocSeg), 1024, &d.sieve_per_sm);
+    if (d.sieve_per_sm < 1) d.sieve_per_sm = 1;
+    d.status = DR_OK;
+}
+
+int count_primes_upto(int64_t x) {  // over the static host list
+    int lo = 0, hi = g_host_prime_count;
+    while (lo < hi) {
+        const int mid = (lo + hi) / 2;
+        if ((int64_t)g_host_primes[mid] <= x) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+int64_t isqrt_exact(int64_t n) {
+    if (n <= 0) return 0;
+    uint64_t s = (uint64_t)std::sqrt((double)n);
+    while ((s + 1) * (s + 1) <= (uint64_t)n) ++s;
+    while (s * s > (uint64_t)n) --s;
+    return (int64_t)s;
+}
+
+}  // namespace
+
+extern "C" int dr_table_build_noalloc(int device, void* stream, int64_t u_total, int64_t u_dense, int64_t mu_limit,
+                                      int16_t* dM, void* planes, int32_t* ckpt, void* wheel) {
+    if (device < 0 || device >= kMaxDevices) return noalloc_fail(DR_ERR_ARG, "device index out of range");
+    if (u_total < 1 || u_total > DR_NOALLOC_MAX_U)
+        return noalloc_fail(DR_ERR_ARG, "u_total must be in [1, DR_NOALLOC_MAX_U = 2^33]");
+    if (u_dense < 0 || u_dense > u_total) return noalloc_fail(DR_ERR_ARG, "u_dense must be in [0, u_total]");
+    if (u_dense > 7600000000LL) return noalloc_fail(DR_ERR_ARG, "u_dense exceeds the int16 prefix range (7.6e9)");
+    if (mu_limit < 0 || mu_limit > u_total) return noalloc_fail(DR_ERR_ARG, "mu_limit must be in [0, u_total]");
+    const int64_t comp = u_total - u_dense;
+    const int64_t nwords = (comp + 63) / 64;
+    if ((u_dense > 0 && !dM) || (nwords > 0 && (!planes || !ckpt)) || !wheel)
+        return noalloc_fail(DR_ERR_ARG, "a table buffer is NULL");
+    if (((uintptr_t)dM & 15) || ((uintptr_t)planes & 15) || ((uintptr_t)wheel & 15) || ((uintptr_t)ckpt & 3))
+        return noalloc_fail(DR_ERR_ARG, "dM, planes and wheel must be 16-byte aligned, ckpt 4-byte aligned");
+
+    int prev = -1;
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e != cudaSuccess) return noalloc_fail(DR_ERR_CUDA, "cudaGetDevice failed", e);
+    if (prev != device && (e = cudaSetDevice(device)) != cudaSuccess)
+        return noalloc_fail(DR_ERR_CUDA, "cudaSetDevice failed", e);
+    DeviceSetup& d = g_dev[device];
+    std::call_once(d.once, setup_device, device, std::ref(d));
+    int rc = d.status;
+    if (rc == DR_OK) {
+        cudaStream_t s = (cudaStream_t)stream;
+        const int S = kNoAllocSeg;
+        const int64_t dense_segs = (u_dense + S - 1) / S;
+        const int64_t nseg = dense_segs + (comp + S - 1) / S;
+        const int64_t root = isqrt_exact(u_total);
+        SieveArgs a;
+        a.u_total = u_total;
+        a.u_dense = u_dense;
+        a.mu_limit = mu_limit;
+        a.dense_segs = dense_segs;
+        a.nseg = nseg;
+        a.S = S;
+        a.n_primes = count_primes_upto(root);
+        a.sq_first = std::min(a.n_primes, count_primes_upto(4));
+        a.w_first = std::min(a.n_primes, count_primes_upto(12));
+        a.tierB_first = std::max(a.w_first, std::min(a.n_primes, count_primes_upto(S / 64 - 1)));
+        a.primes = d.scratch + kOffPrimes;
+        a.stencil4 = d.scratch + kOffStencil;
+        a.dM = dM;
+        a.planes = (ulonglong2*)planes;
+        a.ckpt = ckpt;
+        a.wheel = (uint4*)wheel;
+        a.seg_sum = (int32_t*)(d.scratch + kOffSegSum);
+        int32_t* seg_off = (int32_t*)(d.scratch + kOffSegOff);
+        const int64_t wheel_groups = mu_limit / 192 + 2;
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(nseg, (int64_t)d.sm_count * d.sieve_per_sm));
+        // the wheel is OR-ed into, so it must start at zero; everything in the
+        // scratch that this call reads it also writes first
+        e = cudaMemsetAsync(wheel, 0, (size_t)wheel_groups * 16, s);
+        if (e == cudaSuccess) {
+            launch_sieve(a, grid, 1024, sieve_smem_bytes(S), s);
+            launch_seg_scan(a.seg_sum, seg_off, nseg, s);
+            launch_fixup(dM, u_dense, S, seg_off, ckpt, nwords, dense_segs, d.sm_count, s);
+            e = cudaGetLastError();
+        }
+        if (e != cudaSuccess) rc = noalloc_fail(DR_ERR_CUDA, "table build launch failed", e);
+    }
+    if (prev >= 0 && prev != device) cudaSetDevice(prev);
+    return rc;
+}

@@ -134,6 +134,7 @@ def lib():
             "dr_debug_udiv": (i32, [vp, ctypes.POINTER(u64), ctypes.POINTER(u64), i64, ctypes.POINTER(u64)]),
             "dr_debug_piece": (i32, [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(u64), i64,
                                      ctypes.POINTER(i64)]),
+            "dr_table_build_noalloc": (i32, [i32, vp, i64, i64, i64, vp, vp, vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -150,7 +151,7 @@ def exported_symbols() -> list:
         "dr_ctx_create", "dr_ctx_destroy", "dr_last_error", "dr_ctx_set_hbm_budget", "dr_device_info",
         "dr_default_params", "dr_check_params", "dr_table_bytes", "dr_mertens", "dr_mertens_batch",
         "dr_batch_checksums", "dr_table_build", "dr_table_read", "dr_table_read_wheel", "dr_table_checksums",
-        "dr_debug_udiv", "dr_debug_piece",
+        "dr_debug_udiv", "dr_debug_piece", "dr_table_build_noalloc",
     ]
 
 

@@ -126,6 +126,38 @@ int dr_table_read_wheel(dr_ctx *ctx, int64_t first, int64_t count, int8_t *mu);
 int dr_debug_udiv(dr_ctx *ctx, const uint64_t *y, const uint64_t *d, int64_t n, uint64_t *q);
 int dr_debug_piece(dr_ctx *ctx, const int32_t *piece, const uint64_t *q, int64_t n, int64_t *out);
 
+/* Table build that allocates nothing.  It has no counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc/cudaFree: code whose device memory
+ * belongs to its own allocator (a framework's caching allocator, a pool
+ * reserved at start-up) or that must not allocate once it is serving.  The
+ * caller passes the four table buffers it allocated itself.  The build's
+ * scratch -- per-segment Mobius sums and their offsets, the sieving primes,
+ * the periodic stencil -- is one fixed 616,624-byte __device__ array inside
+ * libdrb200.so, which every GPU that loads the library holds until the
+ * process exits.
+ *
+ *   u_total in [1, DR_NOALLOC_MAX_U = 2^33]; larger sizes are rejected with
+ *   DR_ERR_ARG and a message in dr_last_error().  0 <= u_dense <= u_total
+ *   (and <= 7.6e9), 0 <= mu_limit <= u_total.  Buffers, with W =
+ *   ceil((u_total - u_dense) / 64):
+ *     dM     int16[u_dense], dM[i] = M(i + 1)          16-byte aligned
+ *     planes 16*W bytes: per 64 values {nonzero, negative} bit words
+ *     ckpt   int32[W]: M just before each 64-value word
+ *     wheel  16*(mu_limit/192 + 2) bytes, zeroed by the call, 16-byte aligned
+ * The result equals dr_table_build()'s table.  Work is queued on `stream` (a
+ * cudaStream_t; NULL is the default stream) and the call returns without
+ * waiting: the table is ready when the stream is.  The first call on a device
+ * sets up the scratch for that device (it looks up the array's device address
+ * and copies the primes and the stencil into it, synchronously); make that
+ * first call before any stream capture.  All calls share the one scratch
+ * array, which keeps the last call's contents, so calls whose work overlaps on
+ * the GPU (other streams, other threads) race on it: serialise them. */
+#define DR_NOALLOC_MAX_U 8589934592LL
+int dr_table_build_noalloc(int device, void *stream, int64_t u_total, int64_t u_dense,
+                           int64_t mu_limit, int16_t *dM, void *planes, int32_t *ckpt,
+                           void *wheel);
+
 #ifdef __cplusplus
 }
 #endif
