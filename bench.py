@@ -194,6 +194,35 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
+KNOWN = {10**k: m for k, m in [(9, -222), (10, -33722), (11, -87856), (12, 62366), (13, 599582), (14, -875575),
+                                    (15, -3216373), (16, -3195437), (17, -21830254)]}  # test_dr.cpp, test_cuda.cu, README
+
+
+def run_table_only(args, eng, stream):
+    """Time the table build alone (sieve + prefix + compressed tier): --table u_total[,u_dense[,mu_limit]]."""
+    import torch
+
+    import dr_b200
+
+    parts = [int(float(v)) for v in args.table.split(",")]
+    ut = parts[0]
+    ud = parts[1] if len(parts) > 1 else min(ut, 7600000000)
+    ml = parts[2] if len(parts) > 2 else min(ut, 135001000)
+    tun = dr_b200.Params(segment_log2=args.seg, block_threads=args.block)
+    for _ in range(args.warmup):
+        eng.table_build(ut, ud, ml, tun)
+    ms = []
+    for _ in range(args.steps):
+        ms.append(eng.table_build(ut, ud, ml, tun).table_ms)
+    torch.cuda.synchronize()
+    out_bytes = 2 * ud + 20 * ((ut - ud + 63) // 64) + 16 * (ml // 192 + 2)
+    t = statistics.median(ms) / 1e3
+    peak, kind = load_peaks()
+    print(json.dumps({"metric": "table build", "u_total": ut, "u_dense": ud, "mu_limit": ml, "seg_log2": args.seg,
+                      "block": args.block, "ms": t * 1e3, "values_per_s": ut / t,
+                      "write_GBps": out_bytes / t / 1e9, "hbm_frac": out_bytes / t / 1e9 / peak, "peak_kind": kind}))
+
+
 def run_engine(args, world, rank, local):
     import torch
 
@@ -202,14 +231,21 @@ def run_engine(args, world, rank, local):
     torch.cuda.set_device(local)
     stream = torch.cuda.current_stream()
     eng = dr_b200.Engine(local, stream.cuda_stream)
-    X = X_HEADLINE
+    if args.table:
+        run_table_only(args, eng, stream)
+        eng.close()
+        return
+    X = int(float(args.x)) if "e" in str(args.x) else int(args.x)
+    want = KNOWN.get(X)
     p = dr_b200.default_params(X, dr_b200.POLICY_REFERENCE if args.policy == "reference" else dr_b200.POLICY_GPU)
+
+    def check(m):
+        if want is not None and m != want:
+            raise SystemExit(f"M({X}) mismatch: {m} != {want}")
 
     # warm-up (also the correctness gate)
     for _ in range(args.warmup):
-        r = eng.mertens(X, p)
-        if r.M != M_HEADLINE:
-            raise SystemExit(f"M(10^16) mismatch: {r.M}")
+        check(eng.mertens(X, p).M)
 
     clocks = ClockSampler(local)
     barrier(world)
@@ -222,8 +258,7 @@ def run_engine(args, world, rank, local):
     for _ in range(args.steps):
         r = eng.mertens(X, p)
         stats.append(r.stats)
-        if r.M != M_HEADLINE:
-            raise SystemExit(f"M(10^16) mismatch: {r.M}")
+        check(r.M)
     ev1.record(stream)
     torch.cuda.synchronize()
     host_dt = time.perf_counter() - host_t0
@@ -283,10 +318,10 @@ def run_engine(args, world, rank, local):
         achieved = alg / (sums / 1e3) / 1e9
         kernel = "sums_kernel"
     line = {
-        "metric": "sec per M(10^16)", "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "metric": "sec per M(10^16)" if X == X_HEADLINE else f"sec per M({X})", "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": sec_per * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "int64", "data": "synthetic (the single input X=10^16)",
-        "config": {"workload": f"M(10^16), {args.policy} parameters", "X": X, "u_total": p.u_total,
+        "config": {"workload": f"M({X}), {args.policy} parameters", "X": X, "u_total": p.u_total,
                    "u_dense": p.u_dense, "cx": p.cx, "mu_limit": p.mu_limit,
                    "l2": "inputs larger than L2 (table rebuilt each step)", "parallelism": f"replicas x{world}"},
         "phases_ms": phases,
@@ -312,6 +347,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--policy", choices=["reference", "gpu"], default="reference")
+    ap.add_argument("--x", default="1e16", help="X of the single-query workload (profiling cases)")
+    ap.add_argument("--table", default=None, help="time the table build only: u_total[,u_dense[,mu_limit]]")
+    ap.add_argument("--seg", type=int, default=0, help="sieve segment = 2^seg values (0: default)")
+    ap.add_argument("--block", type=int, default=0, help="sieve threads per CTA (0: default)")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -47,6 +47,15 @@ __device__ __forceinline__ u64 udiv_u64_u32(u64 y, uint32_t d, float inv) {
     return q;
 }
 
+// floor(y / n) from a tabulated reciprocal inv = floor((2^64 - 1) / n), n >= 1.
+// q' = umulhi(y, inv) satisfies y/n - 2 < q' <= floor(y/n) (inv undershoots
+// 2^64/n by less than 1 + 1/n), so one integer correction makes it exact.
+__device__ __forceinline__ u64 udiv_inv(u64 y, u64 n, u64 inv) {
+    const u64 q = __umul64hi(y, inv);
+    const u64 r = y - q * n;
+    return q + (r >= n ? 1ull : 0ull);
+}
+
 __device__ __forceinline__ u64 udiv(u64 y, u64 d) {
     if (d >> 32) return y / d;  // divisor above 32 bits: rare, exact library path
     if ((y >> 32) == 0) return (uint32_t)y / (uint32_t)d;
@@ -96,8 +105,16 @@ __host__ __device__ constexpr PieceCoef make_piece_coef(int piece) {
 }
 
 __device__ __forceinline__ i64 piece_eval(const PieceCoef& c, u64 q) {
-    const u64 k = q / 12u;
-    const uint32_t r = (uint32_t)(q - k * 12u);
+    u64 k;
+    uint32_t r;
+    if ((q >> 32) == 0) {  // most S2 quotients: 32-bit division by the constant 12
+        const uint32_t q32 = (uint32_t)q, k32 = q32 / 12u;
+        k = k32;
+        r = q32 - k32 * 12u;
+    } else {
+        k = q / 12u;
+        r = (uint32_t)(q - k * 12u);
+    }
     const int t = (int)((c.packed >> (5 * r)) & 31u) - 16;
     return c.a * (i64)k + t;
 }

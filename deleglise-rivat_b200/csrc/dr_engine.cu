@@ -68,15 +68,16 @@ struct dr_ctx {
     uint64_t budget = 0;
     uint64_t held = 0;
     // table buffers
-    DevBuf dM, planes, ckpt, wheel, seg_sum, seg_off, primes, stencil;
+    DevBuf dM, planes, ckpt, wheel, seg_sum, seg_off, primes, pinv, items, stencil;
     // query buffers
-    DevBuf queries, ops, prefix, scan_tmp, acc, counts, ticket, misc;
+    DevBuf queries, ops, prefix, scan_tmp, acc, counts, ticket, misc, inv, invw;
     // table state
     bool table_valid = false;
     int64_t t_u_total = 0, t_u_dense = 0, t_mu_limit = 0, t_nwords = 0;
     int t_S = 0;
     // host
     std::vector<uint32_t> host_primes;
+    std::vector<uint64_t> host_pinv;  // per prime: floor((2^64-1)/p), then floor((2^64-1)/p^2)
     int64_t host_primes_root = -1;
     uint64_t* pinned = nullptr;  // 3 * pinned_q u64 + counts
     size_t pinned_cap = 0;
@@ -134,6 +135,13 @@ const std::vector<uint32_t>& primes_upto(dr_ctx* c, int64_t root) {
         }
     }
     c->host_primes_root = root;
+    const size_t np = c->host_primes.size();
+    c->host_pinv.assign(2 * np, 0);
+    for (size_t i = 0; i < np; ++i) {
+        const uint64_t p = c->host_primes[i];
+        c->host_pinv[i] = ~0ull / p;
+        c->host_pinv[np + i] = ~0ull / (p * p);
+    }
     return c->host_primes;
 }
 
@@ -228,7 +236,11 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     if ((rc = ensure(c, c->seg_off, (size_t)nseg * 4))) return rc;
     const std::vector<uint32_t>& pr = primes_upto(c, isqrt_i64(u_total));
     if ((rc = ensure(c, c->primes, pr.size() * 4))) return rc;
-    if (!pr.empty()) CU(cudaMemcpyAsync(c->primes.p, pr.data(), pr.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    if ((rc = ensure(c, c->pinv, pr.size() * 16))) return rc;
+    if (!pr.empty()) {
+        CU(cudaMemcpyAsync(c->primes.p, pr.data(), pr.size() * 4, cudaMemcpyHostToDevice, c->stream));
+        CU(cudaMemcpyAsync(c->pinv.p, c->host_pinv.data(), pr.size() * 16, cudaMemcpyHostToDevice, c->stream));
+    }
 
     SieveArgs a;
     a.u_total = u_total;
@@ -243,8 +255,21 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     };
     a.sq_first = first_at_least(5);
     a.w_first = first_at_least(13);
-    a.tierB_first = std::max(a.w_first, first_at_least((uint32_t)std::max(13, S / 64)));
+    a.tierB_first = std::max(a.w_first, first_at_least((uint32_t)std::max(13, S / 32)));
+    {
+        // first prime whose square reaches S/32
+        int k = a.sq_first;
+        while (k < (int)pr.size() && (uint64_t)pr[k] * pr[k] < (uint64_t)(S / 32)) ++k;
+        a.sqB_first = k;
+    }
+    std::vector<uint4> items(kMaxSieveItems);
+    a.n_items = build_sieve_items(pr.data(), (int)pr.size(), S, items.data(), kMaxSieveItems);
+    if ((rc = ensure(c, c->items, (size_t)std::max(a.n_items, 1) * 16))) return rc;
+    if (a.n_items) CU(cudaMemcpyAsync(c->items.p, items.data(), (size_t)a.n_items * 16, cudaMemcpyHostToDevice, c->stream));
+    a.items = (const uint4*)c->items.p;
     a.primes = (const uint32_t*)c->primes.p;
+    a.pinv = (const u64*)c->pinv.p;
+    a.sqinv = (const u64*)c->pinv.p + pr.size();
     a.stencil4 = (const uint32_t*)c->stencil.p;
     a.dM = (int16_t*)c->dM.p;
     a.planes = (ulonglong2*)c->planes.p;
@@ -312,6 +337,7 @@ int run_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, int
     int rc;
     std::vector<QueryDev> qs((size_t)nq);
     u64 slots = 0;
+    int64_t inv_limit = 0;  // largest S1 divisor n worth tabulating
     for (int64_t i = 0; i < nq; ++i) {
         QueryDev& q = qs[(size_t)i];
         q.X = (u64)std::max<int64_t>(X[i], 0);
@@ -321,7 +347,14 @@ int run_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, int
         q.nc = num_candidates(q.N);
         q.slot_base = slots;
         slots += 2 * (u64)q.nc;
+        if (q.N > 0) {
+            // S1 divisors stay below kappa_y ~ sqrt(y)/cx and the even correction's
+            // 2*kappa_{y/2} ~ sqrt(2y)/cx; larger n (never expected) fall back to udiv
+            const double b = 1.4143 * std::sqrt((double)X[i]) / P[i].cx + 64.0;
+            inv_limit = std::max<int64_t>(inv_limit, (int64_t)std::min(b, 4.0e9));
+        }
     }
+    const int64_t invw_count = c->t_mu_limit / 6 + 1;  // every S2 j <= A <= mu_limit
     if ((rc = ensure(c, c->queries, (size_t)nq * sizeof(QueryDev)))) return rc;
     if ((rc = ensure(c, c->acc, (size_t)nq * 3 * 8))) return rc;
     if ((rc = ensure(c, c->counts, (size_t)nq * 4 * 8))) return rc;
@@ -329,6 +362,8 @@ int run_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, int
     if ((rc = ensure(c, c->prefix, (size_t)(slots + 1) * 8))) return rc;
     if ((rc = ensure(c, c->scan_tmp, scan_u64_tmp_elems(slots) * 8))) return rc;
     if ((rc = ensure(c, c->ticket, 16))) return rc;
+    if ((rc = ensure(c, c->inv, (size_t)(inv_limit + 1) * 8))) return rc;
+    if ((rc = ensure(c, c->invw, (size_t)invw_count * 16))) return rc;
     const size_t need_pinned = (size_t)nq * 7 + 2;
     if (c->pinned_cap < need_pinned) {
         if (c->pinned) cudaFreeHost(c->pinned);
@@ -346,11 +381,12 @@ int run_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, int
     launch_direct((const QueryDev*)c->queries.p, qn, T, (u64*)c->acc.p, c->stream);
     int launches = 1;
     if (slots > 0) {
+        launch_inverse((u64*)c->inv.p, inv_limit, (ulonglong2*)c->invw.p, invw_count, c->sm_count, c->stream);
         launch_plan((const QueryDev*)c->queries.p, qn, T, slots, (u64*)c->ops.p, (u64*)c->acc.p, (i64*)c->counts.p,
                     c->sm_count, c->stream);
         launch_scan_u64((const u64*)c->ops.p, (u64*)c->prefix.p, slots, (u64*)c->scan_tmp.p,
                         scan_u64_tmp_elems(slots), c->stream);
-        launches += 4;
+        launches += 5;
     }
     CU(cudaGetLastError());
     CU(cudaEventRecord(c->ev[3], c->stream));
@@ -364,6 +400,10 @@ int run_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, int
         sa.ticket = (u64*)c->ticket.p;
         sa.acc = (u64*)c->acc.p;
         sa.chunk_log2 = tuning ? tuning->chunk_log2 : 0;
+        sa.inv = (const u64*)c->inv.p;
+        sa.inv_limit = inv_limit;
+        sa.invw = (const ulonglong2*)c->invw.p;
+        sa.invw_count = invw_count;
         int per_sm = 0;
         sums_kernel_occupancy(256, &per_sm);
         const int grid = c->sm_count * std::max(1, per_sm);
@@ -482,8 +522,9 @@ int dr_ctx_destroy(dr_ctx* c) {
     if (!c) return DR_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    DevBuf* bufs[] = {&c->dM, &c->planes, &c->ckpt, &c->wheel, &c->seg_sum, &c->seg_off, &c->primes, &c->stencil,
-                      &c->queries, &c->ops, &c->prefix, &c->scan_tmp, &c->acc, &c->counts, &c->ticket, &c->misc};
+    DevBuf* bufs[] = {&c->dM, &c->planes, &c->ckpt, &c->wheel, &c->seg_sum, &c->seg_off, &c->primes, &c->pinv, &c->items, &c->stencil,
+                      &c->queries, &c->ops, &c->prefix, &c->scan_tmp, &c->acc, &c->counts, &c->ticket, &c->misc,
+                      &c->inv, &c->invw};
     for (DevBuf* b : bufs) release(c, *b);
     if (c->pinned) cudaFreeHost(c->pinned);
     for (auto& e : c->ev)

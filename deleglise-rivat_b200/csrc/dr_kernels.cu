@@ -80,6 +80,12 @@ __device__ int block_excl_scan(int32_t* a, int n, int32_t* wtot) {
     return total;
 }
 
+// y mod d from a tabulated reciprocal inv = floor((2^64-1)/d) (see udiv_inv)
+__device__ __forceinline__ u64 umod_inv(u64 y, u64 d, u64 inv) {
+    const u64 r = y - __umul64hi(y, inv) * d;
+    return r >= d ? r - d : r;
+}
+
 // Byte-log rule (mertens_dr.hpp:145-171) for value n with accumulator acc.
 __device__ __forceinline__ uint32_t finalize_byte(uint32_t acc, u64 n) {
     if (n <= 2) return n == 1 ? 1u : (n == 2 ? 0xFFu : 0u);  // explicit 1 and 2 (:838-839)
@@ -125,45 +131,67 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
         }
         __syncthreads();
 
-        // 2. square flags for p >= 5 (:824-829); idempotent OR, so order-free
-        for (int i = a.sq_first + tid; i < a.n_primes; i += T) {
+        // 2-3. square flags for p >= 5 (:824-829) and log weights for p >= 13
+        //    (:830-835).  Flags are idempotent ORs; weight bytes stay below 0x80,
+        //    so a 32-bit add of w << 8*(j&3) never carries into a neighbour and
+        //    the order of the marks does not matter.
+        //    Smaller moduli: balanced warp items (lanes stride the multiples).
+        for (int it = warp; it < a.n_items; it += nwarps) {
+            const uint4 I = __ldg(a.items + it);
+            if (I.y >= (uint32_t)len) continue;
+            const uint32_t m = I.x;
+            const bool sq = (I.w >> 31) != 0;
+            const uint32_t pidx = I.w & 0x7fffffffu;
+            const u64 inv = sq ? __ldg(a.sqinv + pidx) : __ldg(a.pinv + pidx);
+            const uint32_t r = (uint32_t)umod_inv((u64)low + I.y, m, inv);
+            uint32_t j = I.y + (r ? m - r : 0u) + (uint32_t)lane * m;
+            const uint32_t jend = min((uint32_t)len, I.y + 1024u * m);
+            if (sq) {
+                for (; j < jend; j += 32u * m) atomicOr(&buf32[j >> 2], 0x80u << ((j & 3) * 8));
+            } else {
+                const uint32_t add = I.z;
+                for (; j < jend; j += 32u * m) atomicAdd(&buf32[j >> 2], add << ((j & 3) * 8));
+            }
+        }
+        //    Larger moduli (at most 32 hits per segment): one prime per thread.
+        for (int i = a.sqB_first + tid; i < a.n_primes; i += T) {
             const u64 p = a.primes[i];
             const u64 sq = p * p;
             if (sq > (u64)end) break;
-            u64 r;
-            if (sq >> 32) r = (u64)low % sq;
-            else r = umod_u64_u32((u64)low, (uint32_t)sq);
+            const u64 r = umod_inv((u64)low, sq, a.sqinv[i]);
             for (u64 j = r ? sq - r : 0; j < (u64)len; j += sq)
                 atomicOr(&buf32[j >> 2], 0x80u << ((j & 3) * 8));
-        }
-        // 3. log weights for p >= 13 (:830-835).  The byte sum stays below 0x80,
-        //    so a 32-bit add of w << 8*(j&3) never carries into a neighbour.
-        for (int i = a.w_first + warp; i < a.tierB_first; i += nwarps) {
-            const uint32_t p = a.primes[i];
-            const uint32_t w = (32u - __clz(p - 1)) | 1u;
-            const uint32_t r = umod_u64_u32((u64)low, p);
-            const uint32_t first = r ? p - r : 0;
-            for (uint32_t j = first + lane * p; j < (uint32_t)len; j += 32u * p)
-                atomicAdd(&buf32[j >> 2], w << ((j & 3) * 8));
         }
         for (int i = a.tierB_first + tid; i < a.n_primes; i += T) {
             const uint32_t p = a.primes[i];
             const uint32_t w = (32u - __clz(p - 1)) | 1u;
-            const uint32_t r = umod_u64_u32((u64)low, p);
+            const uint32_t r = (uint32_t)umod_inv((u64)low, p, a.pinv[i]);
             for (uint32_t j = r ? p - r : 0; j < (uint32_t)len; j += p)
                 atomicAdd(&buf32[j >> 2], w << ((j & 3) * 8));
         }
         __syncthreads();
 
-        // 4. finalize to mu bytes in place; bytes past len become 0
+        // 4. finalize to mu bytes in place, four at a time with byte-SIMD
+        //    compares (all four share floor(log2 n) unless the word straddles a
+        //    power of two); bytes past len become 0
         for (int i = tid; i < nw16; i += T) {
             const uint32_t v = buf32[i];
-            uint32_t o = 0;
+            const u64 n0 = (u64)(low + 4 * i);
+            uint32_t o;
+            const int bw0 = 64 - __clzll(n0), bw3 = 64 - __clzll(n0 + 3);
+            if (n0 >= 3 && bw0 == bw3) {
+                const uint32_t thr = (uint32_t)(bw0 - 1) * 0x01010101u;
+                const uint32_t sieved = __vcmpgtu4(v & 0x7F7F7F7Fu, thr);  // every factor sieved
+                const uint32_t odd = __vcmpne4(v & 0x01010101u, 0u);
+                o = ((~(sieved ^ odd)) & 0xFEFEFEFEu) | 0x01010101u;       // -1 if odd == sieved_all
+                o &= __vcmpeq4(v & 0x80808080u, 0u);                        // square factor: 0
+            } else {
+                o = 0;
 #pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                const int idx = 4 * i + b;
-                if (idx < len) o |= finalize_byte((v >> (8 * b)) & 0xFFu, (u64)(low + idx)) << (8 * b);
+                for (int b = 0; b < 4; ++b) o |= finalize_byte((v >> (8 * b)) & 0xFFu, n0 + b) << (8 * b);
             }
+            const int rem = len - 4 * i;
+            if (rem < 4) o = rem <= 0 ? 0u : (o & ((1u << (8 * rem)) - 1u));
             buf32[i] = o;
         }
         __syncthreads();
@@ -249,6 +277,31 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
         if (tid == 0) a.seg_sum[seg] = total;
         __syncthreads();
     }
+}
+
+int build_sieve_items(const uint32_t* primes, int n_primes, int S, uint4* out, int cap) {
+    const uint32_t lim = (uint32_t)(S / 32);
+    int n = 0;
+    for (int i = 0; i < n_primes; ++i) {
+        const uint32_t p = primes[i];
+        if (p >= 13 && p < lim) {
+            const uint32_t w = (32u - (uint32_t)__builtin_clz(p - 1)) | 1u;
+            for (uint32_t st = 0; st < (uint32_t)S; st += 1024u * p)
+                if (n < cap) out[n++] = make_uint4(p, st, w, (uint32_t)i);
+        }
+        if (p >= 5 && p * p < lim) {
+            const uint32_t q = p * p;
+            for (uint32_t st = 0; st < (uint32_t)S; st += 1024u * q)
+                if (n < cap) out[n++] = make_uint4(q, st, 0x80u, (uint32_t)i | 0x80000000u);
+        }
+    }
+    return n;
+}
+
+int sieve_items_prefix(const uint4* items, int n_items, int n_primes) {
+    int k = 0;
+    while (k < n_items && (int)(items[k].w & 0x7fffffffu) < n_primes) ++k;
+    return k;
 }
 
 void sieve_kernel_attrs(size_t smem, int block, int* per_sm) {
@@ -467,36 +520,92 @@ void launch_scan_u64(const u64* in, u64* out, u64 n, u64* tmp, size_t, cudaStrea
 // Persistent S1 / S2 kernel over the flattened op space.
 // ---------------------------------------------------------------------------
 
-// sum of M(floor(y/n)) over n = n0 + stride*i, i in [i0, i1), lanes interleaved
-__device__ __forceinline__ i64 s1_part(const TableView& T, u64 y, i64 n0, int stride, u64 i0, u64 i1, int lane) {
+constexpr int kS1Unroll = 4;  // independent gathers in flight per lane
+constexpr int kS2Unroll = 2;
+
+// sum of M(floor(y/n)) over n = n0 + stride*i, i in [i0, i1), lanes interleaved.
+// Groups of kS1Unroll iterations issue their reciprocal loads, quotients and
+// table gathers back to back; a group whose divisors are all tabulated and
+// whose quotients all fall in the dense tier takes the branch-free path.
+__device__ __forceinline__ i64 s1_part(const SumsArgs& a, u64 y, i64 n0, int stride, u64 i0, u64 i1, int lane) {
     i64 acc = 0;
-    for (u64 i = i0 + lane; i < i1; i += 32) {
+    const u64 lim = (u64)a.inv_limit;
+    const u64 ud = (u64)a.T.u_dense;
+    const u64 nstep = 32ull * (u64)stride;
+    u64 i = i0 + lane;
+    for (; i + 32 * (kS1Unroll - 1) < i1; i += 32 * kS1Unroll) {
+        const u64 nfirst = (u64)n0 + (u64)stride * i;
+        const u64 nlast = nfirst + nstep * (kS1Unroll - 1);
+        if (nlast <= lim) {
+            u64 iv[kS1Unroll], q[kS1Unroll];
+#pragma unroll
+            for (int k = 0; k < kS1Unroll; ++k) iv[k] = __ldg(a.inv + nfirst + nstep * k);
+#pragma unroll
+            for (int k = 0; k < kS1Unroll; ++k) q[k] = udiv_inv(y, nfirst + nstep * k, iv[k]);
+            if (q[0] <= ud && q[kS1Unroll - 1] >= 1) {  // q falls with n: all in the dense tier
+                int32_t m[kS1Unroll];
+#pragma unroll
+                for (int k = 0; k < kS1Unroll; ++k) m[k] = __ldg(a.T.dM + (q[k] - 1));
+#pragma unroll
+                for (int k = 0; k < kS1Unroll; ++k) acc += m[k];
+            } else {
+#pragma unroll
+                for (int k = 0; k < kS1Unroll; ++k) acc += table_M(a.T, q[k]);
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kS1Unroll; ++k) {
+                const u64 n = nfirst + nstep * k;
+                acc += table_M(a.T, n <= lim ? udiv_inv(y, n, __ldg(a.inv + n)) : udiv(y, n));
+            }
+        }
+    }
+    for (; i < i1; i += 32) {
         const u64 n = (u64)n0 + (u64)stride * i;
-        const u64 q = udiv(y, n);
-        acc += table_M(T, q);
+        acc += table_M(a.T, n <= lim ? udiv_inv(y, n, __ldg(a.inv + n)) : udiv(y, n));
+    }
+    return acc;
+}
+
+// mu(j) * piece(floor(y/j)) for one wheel position m (j = 6m+1, 6m+5 within [jlo, jhi])
+__device__ __forceinline__ u64 s2_position(const SumsArgs& a, u64 y, const PieceCoef& pc, i64 jlo, i64 jhi, u64 m,
+                                           const uint4 w, const ulonglong2 iv) {
+    const uint32_t b = (uint32_t)(m & 31u);
+    const i64 j1 = (i64)(6 * m + 1), j5 = (i64)(6 * m + 5);
+    u64 acc = 0;
+    if (((w.x >> b) & 1u) && j1 >= jlo && j1 <= jhi) {
+        const i64 v = piece_eval(pc, udiv_inv(y, (u64)j1, iv.x));
+        acc += ((w.y >> b) & 1u) ? (u64)(-v) : (u64)v;
+    }
+    if (((w.z >> b) & 1u) && j5 >= jlo && j5 <= jhi) {
+        const i64 v = piece_eval(pc, udiv_inv(y, (u64)j5, iv.y));
+        acc += ((w.w >> b) & 1u) ? (u64)(-v) : (u64)v;
     }
     return acc;
 }
 
 // sum of mu(j) * piece(floor(y/j)) for j in {6m+1, 6m+5} within [jlo, jhi],
 // m = jlo/6 + i, i in [i0, i1)
-__device__ __forceinline__ u64 s2_part(const TableView& T, u64 y, const PieceCoef pc, i64 jlo, i64 jhi, u64 i0, u64 i1,
-                                       int lane) {
+__device__ __forceinline__ u64 s2_part(const SumsArgs& a, u64 y, const PieceCoef pc, i64 jlo, i64 jhi, u64 i0,
+                                       u64 i1, int lane) {
     u64 acc = 0;
     const u64 m0 = (u64)(jlo / 6);
-    for (u64 i = i0 + lane; i < i1; i += 32) {
+    u64 i = i0 + lane;
+    for (; i + 32 * (kS2Unroll - 1) < i1; i += 32 * kS2Unroll) {
+        uint4 w[kS2Unroll];
+        ulonglong2 iv[kS2Unroll];
+#pragma unroll
+        for (int k = 0; k < kS2Unroll; ++k) {
+            const u64 m = m0 + i + 32 * k;
+            w[k] = __ldg(a.T.wheel + (m >> 5));
+            iv[k] = __ldg(a.invw + m);
+        }
+#pragma unroll
+        for (int k = 0; k < kS2Unroll; ++k) acc += s2_position(a, y, pc, jlo, jhi, m0 + i + 32 * k, w[k], iv[k]);
+    }
+    for (; i < i1; i += 32) {
         const u64 m = m0 + i;
-        const uint4 w = __ldg(T.wheel + (m >> 5));
-        const uint32_t b = (uint32_t)(m & 31u);
-        const i64 j1 = (i64)(6 * m + 1), j5 = (i64)(6 * m + 5);
-        if (((w.x >> b) & 1u) && j1 >= jlo && j1 <= jhi) {
-            const i64 v = piece_eval(pc, udiv(y, (u64)j1));
-            acc += ((w.y >> b) & 1u) ? (u64)(-v) : (u64)v;
-        }
-        if (((w.z >> b) & 1u) && j5 >= jlo && j5 <= jhi) {
-            const i64 v = piece_eval(pc, udiv(y, (u64)j5));
-            acc += ((w.w >> b) & 1u) ? (u64)(-v) : (u64)v;
-        }
+        acc += s2_position(a, y, pc, jlo, jhi, m, __ldg(a.T.wheel + (m >> 5)), __ldg(a.invw + m));
     }
     return acc;
 }
@@ -513,7 +622,9 @@ __device__ __forceinline__ u64 upper_slot(const u64* prefix, u64 n_slots, u64 o)
 }
 
 __global__ void __launch_bounds__(256) sums_kernel(const SumsArgs a) {
+    __shared__ EvalDesc sdesc[8];  // one decoded evaluation per warp
     const int lane = threadIdx.x & 31;
+    EvalDesc& d = sdesc[threadIdx.x >> 5];
     const u64 total = a.prefix[a.n_slots];
     int lg = a.chunk_log2;
     if (lg <= 0) {
@@ -537,10 +648,13 @@ __global__ void __launch_bounds__(256) sums_kernel(const SumsArgs a) {
             while (a.prefix[s + 1] <= o) ++s;
             const u64 sbase = a.prefix[s];
             const int qi = a.nq == 1 ? 0 : query_of_slot(a.queries, a.nq, s);
-            const QueryDev Q = a.queries[qi];
-            const u64 local = s - Q.slot_base;
-            EvalDesc d;
-            decode_eval(Q, a.T, (i64)(local >> 1), (int)(local & 1), d);
+            __syncwarp();
+            if (lane == 0) {
+                const QueryDev Q = a.queries[qi];
+                const u64 local = s - Q.slot_base;
+                decode_eval(Q, a.T, (i64)(local >> 1), (int)(local & 1), d);
+            }
+            __syncwarp();
             if (qi != cur_q) {
                 if (cur_q >= 0) {
                     const u64 t1 = warp_sum_u64(s1), t2 = warp_sum_u64(s2);
@@ -560,21 +674,24 @@ __global__ void __launch_bounds__(256) sums_kernel(const SumsArgs a) {
                 if (lane == 0) atomicOr(a.ticket + 1, 1ull);
                 break;
             }
+            const u64 y = d.y;
+            const i64 coef = d.coef;
+            const int nseg = d.nseg;
             u64 segstart = 0;
-            for (int g = 0; g < d.nseg && segstart < hi; ++g) {
+            for (int g = 0; g < nseg && segstart < hi; ++g) {
                 const u64 cnt = g < 2 ? (u64)d.s1_cnt[g] : (u64)d.mcnt[g - 2];
                 const u64 sb = segstart;
                 segstart += cnt;
                 const u64 a0 = max(lo, sb), a1 = min(hi, segstart);
                 if (a0 >= a1) continue;
                 if (g < 2) {
-                    const i64 part = s1_part(a.T, d.y, d.s1_n0[g], d.s1_stride[g], a0 - sb, a1 - sb, lane);
-                    const i64 sg = d.coef * d.s1_sign[g];
+                    const i64 part = s1_part(a, y, d.s1_n0[g], d.s1_stride[g], a0 - sb, a1 - sb, lane);
+                    const i64 sg = coef * d.s1_sign[g];
                     s1 += sg > 0 ? (u64)part : (u64)(-part);
                 } else {
                     const int p = g - 2;
-                    const u64 part = s2_part(a.T, d.y, c_piece[d.piece0 + p], d.jlo[p], d.jhi[p], a0 - sb, a1 - sb, lane);
-                    s2 += d.coef > 0 ? part : (u64)(0 - part);
+                    const u64 part = s2_part(a, y, c_piece[d.piece0 + p], d.jlo[p], d.jhi[p], a0 - sb, a1 - sb, lane);
+                    s2 += coef > 0 ? part : (u64)(0 - part);
                 }
             }
             o = sbase + hi;
@@ -588,6 +705,21 @@ __global__ void __launch_bounds__(256) sums_kernel(const SumsArgs a) {
             atomicAdd(a.acc + 3 * cur_q + 2, t2);
         }
     }
+}
+
+// inv[n] = floor((2^64-1)/n) for 1 <= n <= inv_limit; invw[m] = {inv(6m+1), inv(6m+5)}.
+__global__ void inverse_kernel(u64* inv, i64 inv_limit, ulonglong2* invw, i64 invw_count) {
+    const i64 stride = (i64)gridDim.x * blockDim.x;
+    const i64 t0 = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    for (i64 n = t0; n <= inv_limit; n += stride) inv[n] = n ? udiv(~0ull, (u64)n) : 0ull;
+    for (i64 m = t0; m < invw_count; m += stride)
+        invw[m] = make_ulonglong2(udiv(~0ull, (u64)(6 * m + 1)), udiv(~0ull, (u64)(6 * m + 5)));
+}
+
+void launch_inverse(u64* inv, i64 inv_limit, ulonglong2* invw, i64 invw_count, int sm_count, cudaStream_t s) {
+    const i64 work = std::max<i64>(inv_limit + 1, invw_count);
+    const int grid = (int)std::min<i64>((work + 255) / 256, (i64)sm_count * 16);
+    inverse_kernel<<<std::max(grid, 1), 256, 0, s>>>(inv, inv_limit, invw, invw_count);
 }
 
 void sums_kernel_occupancy(int block, int* per_sm) {

@@ -18,8 +18,13 @@ struct SieveArgs {
     int n_primes;       // primes <= isqrt(u_total), ascending
     int sq_first;       // first prime >= 5 (square flags)
     int w_first;        // first prime >= 13 (weights)
-    int tierB_first;    // first prime sieved thread-per-prime
+    int tierB_first;    // first prime whose weights are marked thread-per-prime (p >= S/32)
+    int sqB_first;      // first prime whose square is marked thread-per-prime (p^2 >= S/32)
+    int n_items;        // warp work items for the smaller moduli (see build_sieve_items)
+    const uint4* items; // {modulus, start offset, weight or 0x80, prime index | square bit 31}
     const uint32_t* primes;
+    const u64* pinv;           // floor((2^64-1)/p) per prime: segment offsets without division
+    const u64* sqinv;          // floor((2^64-1)/p^2) per prime
     const uint32_t* stencil4;  // 4 copies shifted by 0..3 bytes, kStencilWords each
     int16_t* dM;
     ulonglong2* planes;
@@ -37,9 +42,24 @@ struct SumsArgs {
     u64* ticket;        // [0]: work-queue counter, [1]: error flag; zeroed before launch
     u64* acc;           // [3 * nq]: C, S1, S2
     int chunk_log2;     // 0: chosen on the device from the total
+    const u64* inv;          // inv[n] = floor((2^64-1)/n), 1 <= n <= inv_limit
+    i64 inv_limit;
+    const ulonglong2* invw;  // invw[m] = {inv(6m+1), inv(6m+5)}, m < invw_count
+    i64 invw_count;
 };
 
 void launch_sieve(const SieveArgs& a, int grid, int block, size_t smem, cudaStream_t s);
+
+// Warp work items for the sieve's smaller moduli: the multiples of every prime
+// 13 <= p < S/32 (log weights) and of every square p^2 < S/32, p >= 5 (flags),
+// cut into pieces of at most 1024 hits (32 lanes x 32 strides), so that the
+// warps of a CTA get equal shares of the marking instead of one warp holding
+// p = 13.  Items are ordered by prime index: the items valid for the first n
+// primes are a prefix.  Returns the count written (<= cap).
+constexpr int kMaxSieveItems = 2048;
+int build_sieve_items(const uint32_t* primes, int n_primes, int S, uint4* out, int cap);
+// Number of leading items whose prime index is below n_primes.
+int sieve_items_prefix(const uint4* items, int n_items, int n_primes);
 size_t sieve_smem_bytes(int S);
 void launch_seg_scan(const int32_t* in, int32_t* out, i64 n, cudaStream_t s);
 void launch_fixup(int16_t* dM, i64 u_dense, int S, const int32_t* seg_off, int32_t* ckpt, i64 nwords,
@@ -49,6 +69,8 @@ void launch_plan(const QueryDev* q, int nq, const TableView& T, u64 n_slots, u64
 void launch_scan_u64(const u64* in, u64* out, u64 n, u64* tmp, size_t tmp_elems, cudaStream_t s);
 size_t scan_u64_tmp_elems(u64 n);
 void launch_sums(const SumsArgs& a, int grid, int block, cudaStream_t s);
+// Reciprocal tables shared by every evaluation of a launch.
+void launch_inverse(u64* inv, i64 inv_limit, ulonglong2* invw, i64 invw_count, int sm_count, cudaStream_t s);
 void launch_direct(const QueryDev* q, int nq, const TableView& T, u64* acc, cudaStream_t s);
 void launch_table_read(const TableView& T, i64 first, i64 count, int32_t* M, int8_t* mu, int8_t* wheel_mu,
                        cudaStream_t s);

@@ -38,7 +38,12 @@ constexpr size_t kOffStencil = 0;
 constexpr size_t kOffSegSum = kOffStencil + (size_t)4 * kStencilWords;
 constexpr size_t kOffSegOff = kOffSegSum + (size_t)kNoAllocMaxSegs;
 constexpr size_t kOffPrimes = kOffSegOff + (size_t)kNoAllocMaxSegs;
-constexpr size_t kScratchWords = kOffPrimes + (size_t)kNoAllocMaxPrimes;  // 616,624 bytes
+constexpr size_t kOffPinv = kOffPrimes + (size_t)kNoAllocMaxPrimes;     // u64 reciprocals of p
+constexpr size_t kOffSqinv = kOffPinv + 2 * (size_t)kNoAllocMaxPrimes;  // u64 reciprocals of p^2
+constexpr size_t kOffItems = kOffSqinv + 2 * (size_t)kNoAllocMaxPrimes;   // uint4 sieve work items
+constexpr size_t kScratchWords = kOffItems + 4 * (size_t)kMaxSieveItems;  // 796,848 bytes
+static_assert(kOffPinv % 2 == 0 && kOffSqinv % 2 == 0, "u64 tables need 8-byte alignment");
+static_assert(kOffItems % 4 == 0, "uint4 items need 16-byte alignment");
 
 // The scratch.  In host code this name is only a host-side stand-in for the
 // symbol, never a device address: the device address comes from
@@ -47,17 +52,24 @@ static __device__ __align__(256) uint32_t g_table_scratch[kScratchWords];
 
 // Host-side constant inputs, filled once per process (static storage, no heap).
 uint32_t g_host_primes[kNoAllocMaxPrimes];
+uint64_t g_host_pinv[kNoAllocMaxPrimes];
+uint64_t g_host_sqinv[kNoAllocMaxPrimes];
 int g_host_prime_count = 0;
 uint32_t g_host_stencil[4 * kStencilWords];
+uint4 g_host_items[kMaxSieveItems];
+int g_host_item_count = 0;
 std::once_flag g_host_once;
 
 void fill_host_constants() {
     static uint8_t composite[kNoAllocMaxRoot + 1];
     for (int64_t p = 2; p <= kNoAllocMaxRoot; ++p) {
         if (composite[p]) continue;
+        g_host_pinv[g_host_prime_count] = ~0ull / (uint64_t)p;
+        g_host_sqinv[g_host_prime_count] = ~0ull / (uint64_t)(p * p);
         g_host_primes[g_host_prime_count++] = (uint32_t)p;
         for (int64_t m = p * p; m <= kNoAllocMaxRoot; m += p) composite[m] = 1;
     }
+    g_host_item_count = build_sieve_items(g_host_primes, g_host_prime_count, kNoAllocSeg, g_host_items, kMaxSieveItems);
     // periodic stencil, 4 copies shifted by 0..3 bytes; byte i describes n = i + 1
     auto stencil_byte = [](int i) -> uint32_t {
         const int n = (i % kStencilPeriod) + 1;
@@ -106,6 +118,15 @@ void setup_device(int device, DeviceSetup& d) {
     e = cudaMemcpy(d.scratch + kOffStencil, g_host_stencil, sizeof(g_host_stencil), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
         e = cudaMemcpy(d.scratch + kOffPrimes, g_host_primes, sizeof(uint32_t) * (size_t)g_host_prime_count,
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(d.scratch + kOffPinv, g_host_pinv, sizeof(uint64_t) * (size_t)g_host_prime_count,
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(d.scratch + kOffSqinv, g_host_sqinv, sizeof(uint64_t) * (size_t)g_host_prime_count,
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(d.scratch + kOffItems, g_host_items, sizeof(uint4) * (size_t)g_host_item_count,
                        cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         d.status = noalloc_fail(DR_ERR_CUDA, "filling the table scratch failed", e);
@@ -180,8 +201,13 @@ extern "C" int dr_table_build_noalloc(int device, void* stream, int64_t u_total,
         a.n_primes = count_primes_upto(root);
         a.sq_first = std::min(a.n_primes, count_primes_upto(4));
         a.w_first = std::min(a.n_primes, count_primes_upto(12));
-        a.tierB_first = std::max(a.w_first, std::min(a.n_primes, count_primes_upto(S / 64 - 1)));
+        a.tierB_first = std::max(a.w_first, std::min(a.n_primes, count_primes_upto(S / 32 - 1)));
+        a.sqB_first = std::max(a.sq_first, std::min(a.n_primes, count_primes_upto(isqrt_exact(S / 32 - 1))));
+        a.n_items = sieve_items_prefix(g_host_items, g_host_item_count, a.n_primes);
+        a.items = (const uint4*)(d.scratch + kOffItems);
         a.primes = d.scratch + kOffPrimes;
+        a.pinv = (const u64*)(d.scratch + kOffPinv);
+        a.sqinv = (const u64*)(d.scratch + kOffSqinv);
         a.stencil4 = d.scratch + kOffStencil;
         a.dM = dM;
         a.planes = (ulonglong2*)planes;

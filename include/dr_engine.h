@@ -133,9 +133,9 @@ int dr_debug_piece(dr_ctx *ctx, const int32_t *piece, const uint64_t *q, int64_t
  * reserved at start-up) or that must not allocate once it is serving.  The
  * caller passes the four table buffers it allocated itself.  The build's
  * scratch -- per-segment Mobius sums and their offsets, the sieving primes,
- * the periodic stencil -- is one fixed 616,624-byte __device__ array inside
- * libdrb200.so, which every GPU that loads the library holds until the
- * process exits.
+ * the periodic stencil, per-prime reciprocals and marking work items -- is one
+ * fixed 796,848-byte __device__ array inside libdrb200.so, which every GPU that
+ * loads the library holds until the process exits.
  *
  *   u_total in [1, DR_NOALLOC_MAX_U = 2^33]; larger sizes are rejected with
  *   DR_ERR_ARG and a message in dr_last_error().  0 <= u_dense <= u_total
