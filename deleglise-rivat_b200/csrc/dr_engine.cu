@@ -303,6 +303,7 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     if (st) {
         st->sieve_launches += 1;
         st->kernel_launches += 3;
+        st->h2d_bytes += (uint64_t)pr.size() * 20 + (uint64_t)a.n_items * 16;
     }
     return DR_OK;
 }
@@ -439,6 +440,8 @@ int run_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, int
         cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]);
         st->d2h_ms += ms;
         st->kernel_launches += launches;
+        st->h2d_bytes += (uint64_t)nq * sizeof(QueryDev);
+        st->d2h_bytes += (uint64_t)nq * 7 * 8 + 16;
         const uint64_t* cnt = c->pinned + (size_t)nq * 3;
         for (int64_t i = 0; i < nq; ++i) {
             st->terms += (int64_t)cnt[4 * i + 0];
@@ -564,7 +567,7 @@ int dr_default_params(int64_t X, int policy, dr_params* out) {
         return DR_OK;
     case DR_POLICY_GPU:
         if (X <= 100000LL) ref_dense_params(X, out);
-        else ref_compressed_params(X, out);
+        else gpu_params(X, out);
         return DR_OK;
     }
     return fail(DR_ERR_ARG, "unknown policy %d", policy);

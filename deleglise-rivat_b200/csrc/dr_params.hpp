@@ -128,4 +128,31 @@ inline void ref_compressed_params(int64_t X, dr_params* p) {
     p->mu_limit = std::min(u_total, mu_limit);
 }
 
+// B200 policy (DR_POLICY_GPU), fitted to measured device times over
+// X = 10^12 .. 10^18 (table build ~4 ms per 10^9 values; S1 ~2.2 ms per 10^9
+// lookups; S2 ~3.8 ms per 10^9 wheel positions): the table is far cheaper to
+// build on the GPU than on the CPU, so u is raised to (X / ln ln X)^(2/3)
+// (the reference's fx = 1.0 without its 8e9 cap), cx = 1.2.  u is capped at
+// 2.5e11 values (~80 GB of compressed tier) and never below the endpoints.
+inline void gpu_params(int64_t X, dr_params* p) {
+    params_clear(p);
+    const double cx = 1.2;
+    const double loglogX = std::log(std::max(2.0, std::log((double)X)));
+    int64_t u = (int64_t)std::pow((double)X / loglogX, 2.0 / 3.0);
+    const int64_t S = isqrt_i64(X);
+    u = std::max(u, 3 * S);
+    u = std::min<int64_t>(u, 250000000000LL);
+    u = ((u + 255) / 256) * 256;
+    int64_t endpoint = (int64_t)(cx * std::sqrt((double)X)) + 1000;
+    u = std::max(u, std::max(S + 1000, endpoint));
+    endpoint = (endpoint + 255) & ~255LL;
+    const int64_t u_dense = std::min(u, std::max(endpoint, std::min<int64_t>(128000000LL, ((u / 4 + 255) & ~255LL))));
+    const int64_t N = X / u;
+    const int64_t A_max = (int64_t)(cx * std::sqrt((double)X)) + 1000;
+    p->u_total = u;
+    p->u_dense = u_dense;
+    p->cx = cx;
+    p->mu_limit = std::min(u, std::max(A_max, N + 1000));
+}
+
 }  // namespace drb

@@ -80,6 +80,8 @@ class Stats(ctypes.Structure):
         ("sums_launches", ctypes.c_int32),
         ("kernel_launches", ctypes.c_int32),
         ("reserved", ctypes.c_int32),
+        ("h2d_bytes", ctypes.c_uint64),
+        ("d2h_bytes", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:

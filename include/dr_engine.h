@@ -75,6 +75,7 @@ typedef struct {
     double h2d_ms, d2h_ms;   /* copies (batched inputs / results)              */
     int32_t sieve_launches, sums_launches, kernel_launches;
     int32_t reserved;
+    uint64_t h2d_bytes, d2h_bytes; /* host<->device bytes copied by the call   */
 } dr_stats;
 
 typedef struct {

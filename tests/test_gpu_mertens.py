@@ -90,3 +90,20 @@ def test_bad_params_raise(engine):
     assert ei.value.code == dr_b200.DR_ERR_PARAMS
     # the context stays usable after a rejected call
     assert engine.compute_mertens(10**9) == -222
+
+
+def test_gpu_policy_known_answers(engine):
+    # the B200 policy (larger u, cx = 1.2) gives the same exact values
+    for c in load_golden("kat.json")["cases"]:
+        p = dr_b200.default_params(c["X"], dr_b200.POLICY_GPU)
+        assert dr_b200.check_params(c["X"], p) == 0
+        assert engine.mertens(c["X"], p).M == c["M"], c
+
+
+def test_m1e18(engine):
+    # pinned only by the reference engine's own run (tests/golden/m1e18.json)
+    g = load_golden("m1e18.json")
+    p = dr_b200.default_params(g["X"], dr_b200.POLICY_GPU)
+    r = engine.mertens(g["X"], p)
+    assert r.M == g["M"]
+    assert (r.stats.C - r.stats.S1 - r.stats.S2) % (1 << 64) == g["M"] % (1 << 64)
