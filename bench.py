@@ -288,17 +288,23 @@ def run_engine(args, world, rank, local):
     batch = None
     if not args.no_batch:
         xs = batch_inputs()
-        bp = [dr_b200.default_params(x, dr_b200.POLICY_GPU) for x in xs]
-        got, _ = eng.mertens_batch(xs, bp)
-        t0 = torch.cuda.Event(enable_timing=True)
-        t1 = torch.cuda.Event(enable_timing=True)
-        reps = 3
-        t0.record(stream)
-        for _ in range(reps):
-            got, bst = eng.mertens_batch(xs, bp)
-        t1.record(stream)
-        torch.cuda.synchronize()
-        bs = t0.elapsed_time(t1) / 1e3 / reps
+
+        def batch_time(bp, reps=3):
+            got, _ = eng.mertens_batch(xs, bp)  # eager run; captures the graph
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            for _ in range(reps):
+                got, bst = eng.mertens_batch(xs, bp)  # graph replays
+            t1.record(stream)
+            torch.cuda.synchronize()
+            return t0.elapsed_time(t1) / 1e3 / reps, got, bst
+
+        untuned_s, _, _ = batch_time([dr_b200.default_params(x, dr_b200.POLICY_GPU) for x in xs])
+        tt0 = time.perf_counter()
+        bp, _ = eng.autotune_batch(xs, 24)
+        tune_s = time.perf_counter() - tt0
+        bs, got, bst = batch_time(bp)
         # baseline: 256 sequential plain single-query calls with default parameters
         s0 = torch.cuda.Event(enable_timing=True)
         s1 = torch.cuda.Event(enable_timing=True)
@@ -311,7 +317,12 @@ def run_engine(args, world, rank, local):
             raise SystemExit("batched and single-query results differ")
         batch = {"queries": len(xs), "M_per_s": len(xs) / bs, "s_per_batch": bs,
                  "sequential_plain_M_per_s": len(xs) / ss, "speedup_vs_sequential": ss / bs,
-                 "launches_per_batch": bst.kernel_launches, "seed": BATCH_SEED, "X": "round(10**U), U~U(9,14)"}
+                 "untuned_batch_M_per_s": len(xs) / untuned_s, "launches_per_batch": bst.kernel_launches,
+                 "cuda_graph": True,
+                 "autotune": {"seconds": tune_s, "u_total": bp[0].u_total, "cx": bp[0].cx,
+                              "segment_log2": bp[0].segment_log2, "block_threads": bp[0].block_threads,
+                              "chunk_log2": bp[0].chunk_log2},
+                 "seed": BATCH_SEED, "X": "round(10**U), U~U(9,14)"}
 
     peak, peak_kind = load_peaks()
     s0_ = stats[0]

@@ -84,13 +84,38 @@ struct dr_ctx {
     std::vector<uint64_t> last_sums;
     cudaEvent_t ev[8] = {};
     bool sieve_attr_set = false;
+    // pinned staging for every host->device source of a call (a captured graph
+    // owns its own staging, so replays never read memory a later call reuses)
+    uint8_t* stage = nullptr;
+    size_t stage_cap = 0, stage_used = 0;
+    bool capturing = false;
+    struct Graph {
+        std::vector<int64_t> X;
+        std::vector<dr_params> P;
+        dr_params tune;
+        cudaGraphExec_t exec = nullptr;
+        uint8_t* stage = nullptr;
+        int launches = 0;
+    };
+    std::vector<Graph> graphs;  // replayable batch pipelines, most recent last
+    bool graphs_enabled = true;
 };
 
 namespace {
 
+void drop_graphs(dr_ctx* c) {
+    for (auto& g : c->graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.stage) cudaFreeHost(g.stage);
+    }
+    c->graphs.clear();
+}
+
 int ensure(dr_ctx* c, DevBuf& b, size_t bytes) {
     bytes = std::max<size_t>(bytes, 16);
     if (bytes <= b.cap) return DR_OK;
+    if (c->capturing) return fail(DR_ERR_ARG, "internal: buffer growth during graph capture");
+    drop_graphs(c);  // captured pipelines hold the old addresses
     const size_t rounded = (bytes + 255) & ~size_t(255);
     if (b.p) {
         cudaStreamSynchronize(c->stream);
@@ -120,6 +145,55 @@ void release(dr_ctx* c, DevBuf& b) {
     }
     b.p = nullptr;
     b.cap = 0;
+}
+
+// Timing events: under stream capture an event record must be an explicit
+// graph node (cudaEventRecordExternal); a plain record there is only a
+// dependency marker and the event would never complete.
+cudaError_t record_event(dr_ctx* c, int i) {
+    if (c->capturing) return cudaEventRecordWithFlags(c->ev[i], c->stream, cudaEventRecordExternal);
+    return cudaEventRecord(c->ev[i], c->stream);
+}
+
+float elapsed_ms(dr_ctx* c, int a, int b) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, c->ev[a], c->ev[b]) != cudaSuccess) {
+        cudaGetLastError();  // timing is informational: never leave a sticky error behind
+        ms = 0.f;
+    }
+    return ms;
+}
+
+int stage_reserve(dr_ctx* c, size_t bytes) {
+    c->stage_used = 0;
+    if (bytes <= c->stage_cap) return DR_OK;
+    if (c->capturing) return fail(DR_ERR_ARG, "internal: staging growth during graph capture");
+    if (c->stage) {
+        cudaStreamSynchronize(c->stream);
+        cudaFreeHost(c->stage);
+    }
+    c->stage = nullptr;
+    c->stage_cap = 0;
+    const size_t cap = (bytes + 4095) & ~size_t(4095);
+    if (cudaMallocHost((void**)&c->stage, cap) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DR_ERR_NOMEM, "pinned staging allocation of %zu bytes failed", cap);
+    }
+    c->stage_cap = cap;
+    return DR_OK;
+}
+
+// Copy `bytes` into the pinned staging area and return the pinned copy.
+const void* stage_put(dr_ctx* c, const void* src, size_t bytes) {
+    const size_t at = (c->stage_used + 15) & ~size_t(15);
+    if (at + bytes > c->stage_cap) return nullptr;
+    std::memcpy(c->stage + at, src, bytes);
+    c->stage_used = at + bytes;
+    return c->stage + at;
+}
+
+size_t stage_bytes_for(size_t n_primes, int64_t nq) {
+    return n_primes * 20 + (size_t)kMaxSieveItems * 16 + (size_t)nq * sizeof(QueryDev) + 256;
 }
 
 // Sieving primes up to root, cached per context.
@@ -238,8 +312,11 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     if ((rc = ensure(c, c->primes, pr.size() * 4))) return rc;
     if ((rc = ensure(c, c->pinv, pr.size() * 16))) return rc;
     if (!pr.empty()) {
-        CU(cudaMemcpyAsync(c->primes.p, pr.data(), pr.size() * 4, cudaMemcpyHostToDevice, c->stream));
-        CU(cudaMemcpyAsync(c->pinv.p, c->host_pinv.data(), pr.size() * 16, cudaMemcpyHostToDevice, c->stream));
+        const void* sp = stage_put(c, pr.data(), pr.size() * 4);
+        const void* sv = stage_put(c, c->host_pinv.data(), pr.size() * 16);
+        if (!sp || !sv) return fail(DR_ERR_NOMEM, "internal: staging area too small");
+        CU(cudaMemcpyAsync(c->primes.p, sp, pr.size() * 4, cudaMemcpyHostToDevice, c->stream));
+        CU(cudaMemcpyAsync(c->pinv.p, sv, pr.size() * 16, cudaMemcpyHostToDevice, c->stream));
     }
 
     SieveArgs a;
@@ -265,7 +342,11 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     std::vector<uint4> items(kMaxSieveItems);
     a.n_items = build_sieve_items(pr.data(), (int)pr.size(), S, items.data(), kMaxSieveItems);
     if ((rc = ensure(c, c->items, (size_t)std::max(a.n_items, 1) * 16))) return rc;
-    if (a.n_items) CU(cudaMemcpyAsync(c->items.p, items.data(), (size_t)a.n_items * 16, cudaMemcpyHostToDevice, c->stream));
+    if (a.n_items) {
+        const void* si = stage_put(c, items.data(), (size_t)a.n_items * 16);
+        if (!si) return fail(DR_ERR_NOMEM, "internal: staging area too small");
+        CU(cudaMemcpyAsync(c->items.p, si, (size_t)a.n_items * 16, cudaMemcpyHostToDevice, c->stream));
+    }
     a.items = (const uint4*)c->items.p;
     a.primes = (const uint32_t*)c->primes.p;
     a.pinv = (const u64*)c->pinv.p;
@@ -283,7 +364,7 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     if (per_sm < 1) per_sm = 1;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(nseg, (int64_t)c->sm_count * per_sm));
 
-    CU(cudaEventRecord(c->ev[0], c->stream));
+    CU(record_event(c, 0));
     CU(cudaMemsetAsync(c->wheel.p, 0, (size_t)wheel_groups * 16, c->stream));
     launch_sieve(a, grid, block, smem, c->stream);
     CU(cudaGetLastError());
@@ -292,7 +373,7 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     launch_fixup((int16_t*)c->dM.p, u_dense, S, (const int32_t*)c->seg_off.p, (int32_t*)c->ckpt.p, nwords,
                  dense_segs, c->sm_count, c->stream);
     CU(cudaGetLastError());
-    CU(cudaEventRecord(c->ev[1], c->stream));
+    CU(record_event(c, 1));
 
     c->table_valid = true;
     c->t_u_total = u_total;
@@ -300,11 +381,7 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     c->t_mu_limit = mu_limit;
     c->t_nwords = nwords;
     c->t_S = S;
-    if (st) {
-        st->sieve_launches += 1;
-        st->kernel_launches += 3;
-        st->h2d_bytes += (uint64_t)pr.size() * 20 + (uint64_t)a.n_items * 16;
-    }
+    if (st) st->kernel_launches += 3;
     return DR_OK;
 }
 
@@ -332,9 +409,10 @@ int resolve_params(int64_t X, const dr_params* in, dr_params* out) {
     return dr_default_params(X, DR_POLICY_REFERENCE, out);
 }
 
-// Run a batch of queries on the current table (already built).
-int run_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, int64_t* out, dr_stats* st,
-                const dr_params* tuning) {
+// Enqueue planning and sums for a batch of queries on the current table.
+// Only stream operations: it can run under graph capture.
+int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, const dr_params* tuning,
+                    int* launches_out) {
     int rc;
     std::vector<QueryDev> qs((size_t)nq);
     u64 slots = 0;
@@ -367,15 +445,19 @@ int run_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, int
     if ((rc = ensure(c, c->invw, (size_t)invw_count * 16))) return rc;
     const size_t need_pinned = (size_t)nq * 7 + 2;
     if (c->pinned_cap < need_pinned) {
+        if (c->capturing) return fail(DR_ERR_ARG, "internal: result buffer growth during graph capture");
+        drop_graphs(c);
         if (c->pinned) cudaFreeHost(c->pinned);
         c->pinned = nullptr;
         CU(cudaMallocHost((void**)&c->pinned, need_pinned * 8));
         c->pinned_cap = need_pinned;
     }
+    const void* sq = stage_put(c, qs.data(), (size_t)nq * sizeof(QueryDev));
+    if (!sq) return fail(DR_ERR_NOMEM, "internal: staging area too small");
     const TableView T = view_of(c);
     const int qn = (int)nq;
-    CU(cudaEventRecord(c->ev[2], c->stream));
-    CU(cudaMemcpyAsync(c->queries.p, qs.data(), (size_t)nq * sizeof(QueryDev), cudaMemcpyHostToDevice, c->stream));
+    CU(record_event(c, 2));
+    CU(cudaMemcpyAsync(c->queries.p, sq, (size_t)nq * sizeof(QueryDev), cudaMemcpyHostToDevice, c->stream));
     CU(cudaMemsetAsync(c->acc.p, 0, (size_t)nq * 3 * 8, c->stream));
     CU(cudaMemsetAsync(c->counts.p, 0, (size_t)nq * 4 * 8, c->stream));
     CU(cudaMemsetAsync(c->ticket.p, 0, 16, c->stream));
@@ -390,7 +472,7 @@ int run_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, int
         launches += 5;
     }
     CU(cudaGetLastError());
-    CU(cudaEventRecord(c->ev[3], c->stream));
+    CU(record_event(c, 3));
     if (slots > 0) {
         SumsArgs sa;
         sa.queries = (const QueryDev*)c->queries.p;
@@ -411,14 +493,20 @@ int run_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, int
         launch_sums(sa, grid, 256, c->stream);
         CU(cudaGetLastError());
         launches += 1;
-        if (st) st->sums_launches += 1;
     }
-    CU(cudaEventRecord(c->ev[4], c->stream));
+    CU(record_event(c, 4));
     CU(cudaMemcpyAsync(c->pinned, c->acc.p, (size_t)nq * 3 * 8, cudaMemcpyDeviceToHost, c->stream));
     CU(cudaMemcpyAsync(c->pinned + (size_t)nq * 3, c->counts.p, (size_t)nq * 4 * 8, cudaMemcpyDeviceToHost,
                        c->stream));
     CU(cudaMemcpyAsync(c->pinned + (size_t)nq * 7, c->ticket.p, 16, cudaMemcpyDeviceToHost, c->stream));
-    CU(cudaEventRecord(c->ev[5], c->stream));
+    CU(record_event(c, 5));
+    *launches_out = launches;
+    return DR_OK;
+}
+
+// Wait for the enqueued work and turn the per-query sums into results.
+int finish_queries(dr_ctx* c, const int64_t* X, int64_t nq, int launches, size_t h2d_bytes, int64_t* out,
+                   dr_stats* st) {
     CU(cudaStreamSynchronize(c->stream));
     CU(cudaGetLastError());
     if (c->pinned[(size_t)nq * 7 + 1])
@@ -428,19 +516,18 @@ int run_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, int
         out[i] = X[i] < 1 ? 0 : (int64_t)(a[0] - a[1] - a[2]);
         // X <= u is answered from the table alone: no terms, so no checksums
         // (the reference returns get_M(X) there, mertens_dr.hpp:1465-1467)
-        if (qs[(size_t)i].N == 0) a[0] = a[1] = a[2] = 0;
+        if (X[i] <= c->t_u_total) a[0] = a[1] = a[2] = 0;
     }
     c->last_sums.assign(c->pinned, c->pinned + (size_t)nq * 3);
     if (st) {
-        float ms = 0;
-        cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
-        st->plan_ms += ms;
-        cudaEventElapsedTime(&ms, c->ev[3], c->ev[4]);
-        st->sums_ms += ms;
-        cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]);
-        st->d2h_ms += ms;
+        st->table_ms += elapsed_ms(c, 0, 1);
+        st->plan_ms += elapsed_ms(c, 2, 3);
+        st->sums_ms += elapsed_ms(c, 3, 4);
+        st->d2h_ms += elapsed_ms(c, 4, 5);
         st->kernel_launches += launches;
-        st->h2d_bytes += (uint64_t)nq * sizeof(QueryDev);
+        st->sieve_launches += 1;
+        st->sums_launches += launches > 1 ? 1 : 0;
+        st->h2d_bytes += (uint64_t)h2d_bytes;
         st->d2h_bytes += (uint64_t)nq * 7 * 8 + 16;
         const uint64_t* cnt = c->pinned + (size_t)nq * 3;
         for (int64_t i = 0; i < nq; ++i) {
@@ -457,6 +544,61 @@ int run_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, int
         }
     }
     return DR_OK;
+}
+
+// Capture the whole batch pipeline (table build, planning, sums, result copy)
+// into a CUDA graph for replay by the next identical call.  Runs right after an
+// eager run of the same batch, so no buffer grows during capture.  Failing to
+// capture is not an error: the batch simply keeps running eagerly.
+void capture_graph(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, const dr_params& tune, int64_t ut,
+                   int64_t ud, int64_t ml, size_t n_primes) {
+    if (c->graphs.size() >= 4) {
+        if (c->graphs.front().exec) cudaGraphExecDestroy(c->graphs.front().exec);
+        if (c->graphs.front().stage) cudaFreeHost(c->graphs.front().stage);
+        c->graphs.erase(c->graphs.begin());
+    }
+    dr_ctx::Graph g;
+    g.X.assign(X, X + nq);
+    g.P.assign(P, P + nq);
+    g.tune = tune;
+    const size_t need = stage_bytes_for(n_primes, nq);
+    if (cudaMallocHost((void**)&g.stage, need) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    uint8_t* saved = c->stage;
+    const size_t saved_cap = c->stage_cap, saved_used = c->stage_used;
+    c->stage = g.stage;
+    c->stage_cap = need;
+    c->stage_used = 0;
+    c->capturing = true;
+    int rc = DR_ERR_CUDA;
+    int launches = 0;
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed) == cudaSuccess) {
+        rc = build_table(c, ut, ud, ml, &tune, nullptr);
+        if (rc == DR_OK) rc = enqueue_queries(c, X, P, nq, &tune, &launches);
+        if (cudaStreamEndCapture(c->stream, &graph) != cudaSuccess) rc = DR_ERR_CUDA;
+    }
+    c->capturing = false;
+    c->stage = saved;
+    c->stage_cap = saved_cap;
+    c->stage_used = saved_used;
+    if (rc == DR_OK && graph && cudaGraphInstantiate(&g.exec, graph, 0) == cudaSuccess) {
+        g.launches = launches + 3;
+        c->graphs.push_back(std::move(g));
+    } else {
+        if (g.stage) cudaFreeHost(g.stage);
+    }
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+}
+
+bool same_batch(const dr_ctx::Graph& g, const int64_t* X, const dr_params* P, int64_t nq, const dr_params& tune) {
+    if ((int64_t)g.X.size() != nq) return false;
+    if (std::memcmp(g.X.data(), X, (size_t)nq * 8) != 0) return false;
+    if (std::memcmp(g.P.data(), P, (size_t)nq * sizeof(dr_params)) != 0) return false;
+    return std::memcmp(&g.tune, &tune, sizeof(dr_params)) == 0;
 }
 
 }  // namespace
@@ -529,7 +671,9 @@ int dr_ctx_destroy(dr_ctx* c) {
                       &c->queries, &c->ops, &c->prefix, &c->scan_tmp, &c->acc, &c->counts, &c->ticket, &c->misc,
                       &c->inv, &c->invw};
     for (DevBuf* b : bufs) release(c, *b);
+    drop_graphs(c);
     if (c->pinned) cudaFreeHost(c->pinned);
+    if (c->stage) cudaFreeHost(c->stage);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -598,13 +742,13 @@ int dr_table_build(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit
     if (!c) return fail(DR_ERR_ARG, "ctx is NULL");
     CU(cudaSetDevice(c->device));
     const double t0 = now_ms();
-    int rc = build_table(c, u_total, u_dense, mu_limit, tuning, st);
+    int rc = stage_reserve(c, stage_bytes_for(primes_upto(c, isqrt_i64(std::max<int64_t>(u_total, 0))).size(), 0));
+    if (rc) return rc;
+    rc = build_table(c, u_total, u_dense, mu_limit, tuning, st);
     if (rc) return rc;
     CU(cudaStreamSynchronize(c->stream));
     if (st) {
-        float ms = 0;
-        cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
-        st->table_ms += ms;
+        st->table_ms += elapsed_ms(c, 0, 1);
         st->total_ms += now_ms() - t0;
     }
     return DR_OK;
@@ -643,17 +787,156 @@ int dr_mertens_batch(dr_ctx* c, const int64_t* X, int64_t count, const dr_params
         int rc = check_query(X[i], P[(size_t)i], ut, ml);
         if (rc) return rc;
     }
-    int rc = build_table(c, ut, ud, ml, p ? p : nullptr, st);
-    if (rc) return rc;
-    rc = run_queries(c, X, P.data(), count, out, st, p ? p : nullptr);
-    if (rc) return rc;
-    if (st) {
-        float ms = 0;
-        cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
-        st->table_ms += ms;
-        st->total_ms = now_ms() - t0;
-        if (count == 1) st->M = out[0];
+    // tuning knobs (segment length, block shape, work-item size) come from p[0]
+    dr_params tune;
+    params_clear(&tune);
+    if (p) {
+        tune.segment_log2 = p[0].segment_log2;
+        tune.block_threads = p[0].block_threads;
+        tune.chunk_log2 = p[0].chunk_log2;
     }
+    // a batch seen before replays its captured CUDA graph: one graph launch
+    // rebuilds the table and recomputes every query
+    if (count > 1) {
+        for (auto& g : c->graphs) {
+            if (!same_batch(g, X, P.data(), count, tune)) continue;
+            CU(cudaGraphLaunch(g.exec, c->stream));
+            c->table_valid = true;
+            c->t_u_total = ut;
+            c->t_u_dense = ud;
+            c->t_mu_limit = ml;
+            c->t_nwords = (ut - ud + 63) / 64;
+            int rc = finish_queries(c, X, count, g.launches, stage_bytes_for(c->host_primes.size(), count), out, st);
+            if (rc) return rc;
+            if (st) st->total_ms = now_ms() - t0;
+            return DR_OK;
+        }
+    }
+    const size_t n_primes = primes_upto(c, isqrt_i64(ut)).size();
+    int rc = stage_reserve(c, stage_bytes_for(n_primes, count));
+    if (rc) return rc;
+    rc = build_table(c, ut, ud, ml, &tune, st);
+    if (rc) return rc;
+    int launches = 0;
+    rc = enqueue_queries(c, X, P.data(), count, &tune, &launches);
+    if (rc) return rc;
+    rc = finish_queries(c, X, count, launches, c->stage_used, out, st);
+    if (rc) return rc;
+    if (st) st->total_ms = now_ms() - t0;
+    if (count > 1 && c->graphs_enabled) capture_graph(c, X, P.data(), count, tune, ut, ud, ml, n_primes);
+    return DR_OK;
+}
+
+// One candidate of the batch autotuner: every query shares a table of
+// u = m * (B200-policy u of the largest X) values and uses all of it.
+static int batch_candidate(const int64_t* X, int64_t n, double m, double cx, int seg, int block, int chunk,
+                           std::vector<dr_params>& P) {
+    int64_t xmax = 1;
+    for (int64_t i = 0; i < n; ++i) xmax = std::max(xmax, X[i]);
+    dr_params base;
+    dr_default_params(xmax, DR_POLICY_GPU, &base);
+    int64_t ut = (int64_t)((double)base.u_total * m);
+    ut = std::min<int64_t>(std::max<int64_t>(ut, 64), 250000000000LL);
+    ut = ((ut + 255) / 256) * 256;
+    int64_t amax = 0, nmax = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        if (X[i] < 1) continue;
+        amax = std::max<int64_t>(amax, (int64_t)(cx * std::sqrt((double)X[i])) + 1000);
+        nmax = std::max<int64_t>(nmax, X[i] / ut + 1000);
+    }
+    const int64_t ud = std::min<int64_t>(ut, std::max<int64_t>((amax + 255) & ~255LL, std::min<int64_t>(128000000LL, ((ut / 4 + 255) & ~255LL))));
+    const int64_t ml = std::min(ut, std::max(amax, nmax));
+    P.assign((size_t)n, dr_params{});
+    for (int64_t i = 0; i < n; ++i) {
+        dr_params& q = P[(size_t)i];
+        params_clear(&q);
+        q.u_total = ut;
+        q.u_dense = ud;
+        q.cx = cx;
+        q.mu_limit = ml;
+        q.segment_log2 = seg;
+        q.block_threads = block;
+        q.chunk_log2 = chunk;
+        if (X[i] >= 1 && check_query(X[i], q, ut, ml) != DR_OK) return DR_ERR_PARAMS;
+    }
+    return DR_OK;
+}
+
+int dr_autotune_batch(dr_ctx* c, const int64_t* X, int64_t count, int max_trials, dr_params* out, double* best_ms) {
+    if (!c || !X || !out || count < 1) return fail(DR_ERR_ARG, "bad argument");
+    const bool saved_graphs = c->graphs_enabled;
+    c->graphs_enabled = false;  // trials run eagerly; only the winner is worth a graph
+    std::vector<int64_t> res((size_t)count);
+    struct State { double m, cx; int seg, block, chunk; } cur{1.0, 1.2, 17, 1024, 0}, best_state = cur;
+    double best = 1e300;
+    int trials = 0;
+    if (max_trials <= 0) max_trials = 24;
+    auto eval = [&](const State& st_) -> double {
+        std::vector<dr_params> P;
+        if (batch_candidate(X, count, st_.m, st_.cx, st_.seg, st_.block, st_.chunk, P) != DR_OK) return 1e300;
+        if (dr_check_params(1, &P[0], c->budget / 2) != DR_OK) return 1e300;
+        if (dr_table_bytes(P[0].u_total, P[0].u_dense, P[0].mu_limit) > c->budget / 2) return 1e300;
+        double t = 1e300;
+        for (int rep = 0; rep < 2; ++rep) {
+            dr_stats st;
+            if (dr_mertens_batch(c, X, count, P.data(), res.data(), &st) != DR_OK) return 1e300;
+            t = std::min(t, st.table_ms + st.plan_ms + st.sums_ms);
+        }
+        ++trials;
+        return t;
+    };
+    best = eval(cur);
+    best_state = cur;
+    const double ms[] = {0.25, 0.5, 2.0, 4.0, 8.0, 16.0};
+    const double cxs[] = {0.9, 1.05, 1.4, 1.7};
+    const int segs[] = {15, 16};
+    const int blocks[] = {512};
+    const int chunks[] = {12, 14, 16};
+    for (int pass = 0; pass < 2 && trials < max_trials; ++pass) {
+        for (double v : ms) {
+            if (trials >= max_trials) break;
+            State t = best_state;
+            t.m = v;
+            if (t.m == best_state.m) continue;
+            const double r = eval(t);
+            if (r < best) best = r, best_state = t;
+        }
+        for (double v : cxs) {
+            if (trials >= max_trials) break;
+            State t = best_state;
+            t.cx = v;
+            const double r = eval(t);
+            if (r < best) best = r, best_state = t;
+        }
+        for (int v : segs) {
+            if (trials >= max_trials) break;
+            State t = best_state;
+            t.seg = v;
+            const double r = eval(t);
+            if (r < best) best = r, best_state = t;
+        }
+        for (int v : blocks) {
+            if (trials >= max_trials) break;
+            State t = best_state;
+            t.block = v;
+            const double r = eval(t);
+            if (r < best) best = r, best_state = t;
+        }
+        for (int v : chunks) {
+            if (trials >= max_trials) break;
+            State t = best_state;
+            t.chunk = v;
+            const double r = eval(t);
+            if (r < best) best = r, best_state = t;
+        }
+    }
+    c->graphs_enabled = saved_graphs;
+    std::vector<dr_params> P;
+    if (best >= 1e299 || batch_candidate(X, count, best_state.m, best_state.cx, best_state.seg, best_state.block,
+                                         best_state.chunk, P) != DR_OK)
+        return fail(DR_ERR_PARAMS, "autotune found no valid configuration");
+    std::memcpy(out, P.data(), (size_t)count * sizeof(dr_params));
+    if (best_ms) *best_ms = best;
     return DR_OK;
 }
 

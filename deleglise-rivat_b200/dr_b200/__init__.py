@@ -137,6 +137,7 @@ def lib():
             "dr_debug_piece": (i32, [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(u64), i64,
                                      ctypes.POINTER(i64)]),
             "dr_table_build_noalloc": (i32, [i32, vp, i64, i64, i64, vp, vp, vp, vp]),
+            "dr_autotune_batch": (i32, [vp, ctypes.POINTER(i64), i64, i32, P, ctypes.POINTER(ctypes.c_double)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -153,7 +154,7 @@ def exported_symbols() -> list:
         "dr_ctx_create", "dr_ctx_destroy", "dr_last_error", "dr_ctx_set_hbm_budget", "dr_device_info",
         "dr_default_params", "dr_check_params", "dr_table_bytes", "dr_mertens", "dr_mertens_batch",
         "dr_batch_checksums", "dr_table_build", "dr_table_read", "dr_table_read_wheel", "dr_table_checksums",
-        "dr_debug_udiv", "dr_debug_piece", "dr_table_build_noalloc",
+        "dr_debug_udiv", "dr_debug_piece", "dr_table_build_noalloc", "dr_autotune_batch",
     ]
 
 
@@ -241,6 +242,15 @@ class Engine:
             parr = (Params * n)(*params)
         _check(lib().dr_mertens_batch(self._ctx, arr, n, parr, out, ctypes.byref(st)))
         return list(out), st
+
+    def autotune_batch(self, Xs: Sequence[int], max_trials: int = 24):
+        """Batch autotuner: (per-query Params, best device ms)."""
+        n = len(Xs)
+        arr = (ctypes.c_int64 * n)(*[int(x) for x in Xs])
+        out = (Params * n)()
+        best = ctypes.c_double()
+        _check(lib().dr_autotune_batch(self._ctx, arr, n, int(max_trials), out, ctypes.byref(best)))
+        return list(out), best.value
 
     def batch_checksums(self, n: int):
         buf = (ctypes.c_uint64 * (3 * n))()

@@ -25,7 +25,9 @@
  *                              members dense_M/mu/chunks/checkpoints :681-687 (SieveTable
  *                              :376-457 when u_dense == u_total).
  *   dr_mertens_batch()      <- no counterpart (the reference evaluates one X per call);
- *                              it is the batched mode of compute_mertens.
+ *                              it is the batched mode of compute_mertens.  A batch
+ *                              repeated with identical inputs replays a captured
+ *                              CUDA graph of its whole pipeline.
  */
 #ifndef DR_ENGINE_H
 #define DR_ENGINE_H
@@ -108,6 +110,14 @@ int dr_mertens_batch(dr_ctx *ctx, const int64_t *X, int64_t count, const dr_para
                      int64_t *out, dr_stats *stats);
 /* Per-query checksums of the last batch (count x {C, S1, S2}). */
 int dr_batch_checksums(dr_ctx *ctx, uint64_t *out3, int64_t count);
+/* Batch autotuner -- no counterpart in the reference.  Times the given batch
+ * on the device for up to max_trials configurations (coordinate descent over
+ * the shared table size, cx, sieve segment length and block shape, and the
+ * S1/S2 work-item size) and writes the best one as count dr_params (all
+ * sharing one table) plus its device time.  Every configuration gives the
+ * same exact M(X). */
+int dr_autotune_batch(dr_ctx *ctx, const int64_t *X, int64_t count, int max_trials, dr_params *out,
+                      double *best_ms);
 
 /* Tables (reference: CompressedMertensTable / SieveTable) -------------------- */
 int dr_table_build(dr_ctx *ctx, int64_t u_total, int64_t u_dense, int64_t mu_limit,

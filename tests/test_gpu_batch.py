@@ -40,3 +40,23 @@ def test_batch_mixed_sizes(engine, oracle):
     got, _ = engine.mertens_batch(xs)
     for x, m in zip(xs, got):
         assert m == (oracle.mertens(x) if x > 0 else 0), x
+
+
+def test_batch_graph_replay(engine):
+    # the second identical call replays the captured CUDA graph of the pipeline
+    g = load_golden("batch256.json")
+    ps = [dr_b200.default_params(x, dr_b200.POLICY_GPU) for x in g["X"]]
+    a, _ = engine.mertens_batch(g["X"], ps)
+    b, st = engine.mertens_batch(g["X"], ps)
+    c, _ = engine.mertens_batch(g["X"], ps)
+    assert a == b == c == g["M"]
+    assert st.kernel_launches >= 10
+
+
+def test_autotune_batch(engine):
+    g = load_golden("batch256.json")
+    ps, best = engine.autotune_batch(g["X"], max_trials=10)
+    assert best > 0
+    assert len({(p.u_total, p.u_dense, p.mu_limit) for p in ps}) == 1  # one shared table
+    got, _ = engine.mertens_batch(g["X"], ps)
+    assert got == g["M"]
