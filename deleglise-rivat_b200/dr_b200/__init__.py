@@ -138,6 +138,19 @@ def lib():
                                      ctypes.POINTER(i64)]),
             "dr_table_build_noalloc": (i32, [i32, vp, i64, i64, i64, vp, vp, vp, vp]),
             "dr_autotune_batch": (i32, [vp, ctypes.POINTER(i64), i64, i32, P, ctypes.POINTER(ctypes.c_double)]),
+            "dr_mlp_create": (i32, [vp, u64, ctypes.POINTER(vp)]),
+            "dr_mlp_destroy": (i32, [vp]),
+            "dr_mlp_num_params": (i64, []),
+            "dr_mlp_set_weights": (i32, [vp, ctypes.POINTER(ctypes.c_float), i64]),
+            "dr_mlp_get_weights": (i32, [vp, ctypes.POINTER(ctypes.c_float), i64]),
+            "dr_mlp_forward": (i32, [vp, ctypes.POINTER(ctypes.c_float), i64, ctypes.POINTER(ctypes.c_float)]),
+            "dr_mlp_grad": (i32, [vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), i64,
+                                  ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
+            "dr_mlp_train": (i32, [vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), i64, i32,
+                                   ctypes.c_float, ctypes.POINTER(ctypes.c_float)]),
+            "dr_tuner_features": (i32, [i64, u64, i32, i32, ctypes.POINTER(ctypes.c_float)]),
+            "dr_tuner_params": (i32, [i64, ctypes.POINTER(ctypes.c_float), P]),
+            "dr_tuner_propose": (i32, [vp, i64, u64, i32, i32, P, ctypes.POINTER(i32)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -155,6 +168,8 @@ def exported_symbols() -> list:
         "dr_default_params", "dr_check_params", "dr_table_bytes", "dr_mertens", "dr_mertens_batch",
         "dr_batch_checksums", "dr_table_build", "dr_table_read", "dr_table_read_wheel", "dr_table_checksums",
         "dr_debug_udiv", "dr_debug_piece", "dr_table_build_noalloc", "dr_autotune_batch",
+        "dr_mlp_create", "dr_mlp_destroy", "dr_mlp_num_params", "dr_mlp_set_weights", "dr_mlp_get_weights",
+        "dr_mlp_forward", "dr_mlp_grad", "dr_mlp_train", "dr_tuner_features", "dr_tuner_params", "dr_tuner_propose",
     ]
 
 
@@ -312,3 +327,92 @@ def device_info(device: int = 0):
     hbm = ctypes.c_uint64()
     _check(lib().dr_device_info(int(device), ctypes.byref(sm), ctypes.byref(hbm)))
     return sm.value, hbm.value
+
+
+def _fptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def tuner_features(X: int, budget: int, sms: int = 148, batch: int = 1):
+    import numpy as np
+
+    f = np.zeros(4, dtype=np.float32)
+    _check(lib().dr_tuner_features(int(X), int(budget), int(sms), int(batch), _fptr(f)))
+    return f
+
+
+def tuner_params(X: int, y_normalised) -> Params:
+    import numpy as np
+
+    y = np.ascontiguousarray(y_normalised, dtype=np.float32)
+    p = Params()
+    _check(lib().dr_tuner_params(int(X), _fptr(y), ctypes.byref(p)))
+    return p
+
+
+class MLP:
+    """The learned tuner's network on the device (dr_mlp_*)."""
+
+    def __init__(self, engine: Engine, seed: int = 1):
+        self._h = ctypes.c_void_p()
+        _check(lib().dr_mlp_create(engine._ctx, int(seed), ctypes.byref(self._h)))
+        self.n_params = int(lib().dr_mlp_num_params())
+
+    def close(self):
+        if self._h:
+            lib().dr_mlp_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_weights(self):
+        import numpy as np
+
+        w = np.zeros(self.n_params, dtype=np.float32)
+        _check(lib().dr_mlp_get_weights(self._h, _fptr(w), self.n_params))
+        return w
+
+    def set_weights(self, w):
+        import numpy as np
+
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        _check(lib().dr_mlp_set_weights(self._h, _fptr(w), len(w)))
+
+    def forward(self, x):
+        import numpy as np
+
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.zeros((x.shape[0], 4), dtype=np.float32)
+        _check(lib().dr_mlp_forward(self._h, _fptr(x), x.shape[0], _fptr(y)))
+        return y
+
+    def grad(self, x, t):
+        import numpy as np
+
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        g = np.zeros(self.n_params, dtype=np.float32)
+        loss = ctypes.c_float()
+        _check(lib().dr_mlp_grad(self._h, _fptr(x), _fptr(t), x.shape[0], _fptr(g), ctypes.byref(loss)))
+        return g, loss.value
+
+    def train(self, x, t, steps: int, lr: float = 3e-3) -> float:
+        import numpy as np
+
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        loss = ctypes.c_float()
+        _check(lib().dr_mlp_train(self._h, _fptr(x), _fptr(t), x.shape[0], int(steps), float(lr), ctypes.byref(loss)))
+        return loss.value
+
+    def propose(self, X: int, budget: int, sms: int = 148, batch: int = 1):
+        """(Params, used_fallback) for X: inference + coverage check + fallback."""
+        p = Params()
+        fb = ctypes.c_int()
+        _check(lib().dr_tuner_propose(self._h, int(X), int(budget), int(sms), int(batch), ctypes.byref(p),
+                                      ctypes.byref(fb)))
+        return p, bool(fb.value)

@@ -119,6 +119,36 @@ int dr_batch_checksums(dr_ctx *ctx, uint64_t *out3, int64_t count);
 int dr_autotune_batch(dr_ctx *ctx, const int64_t *X, int64_t count, int max_trials, dr_params *out,
                       double *best_ms);
 
+/* Learned tuner -- no counterpart in the reference (whose parameters come from
+ * the fixed heuristics choose_cx / choose_compressed_limit, mertens_dr.hpp:914,
+ * :1401).  A 4-64-64-4 FP32 MLP on the device with hand-written forward,
+ * backward and Adam kernels.  Inputs: log10 X, log2 HBM budget, SM count,
+ * log2 batch size; outputs: cx, log2 fx, log2 u_cap, log2 segment length with
+ * u = min(fx (X / ln ln X)^(2/3), u_cap); both normalised by fixed affine
+ * maps (dr_tuner_features), inputs clamped to the training domain (log10 X in
+ * [10, 16], budget 8..160 GiB).  4740 parameters in the order W1[64][4] b1[64]
+ * W2[64][64] b2[64] W3[4][64] b3[4]. */
+typedef struct dr_mlp dr_mlp;
+int dr_mlp_create(dr_ctx *ctx, uint64_t seed, dr_mlp **out);
+int dr_mlp_destroy(dr_mlp *mlp);
+int64_t dr_mlp_num_params(void);
+int dr_mlp_set_weights(dr_mlp *mlp, const float *w, int64_t count);
+int dr_mlp_get_weights(dr_mlp *mlp, float *w, int64_t count);
+/* Forward pass on B normalised feature rows (B x 4 -> B x 4, host arrays). */
+int dr_mlp_forward(dr_mlp *mlp, const float *x, int64_t B, float *y);
+/* Gradient of the mean squared error over B examples (no update). */
+int dr_mlp_grad(dr_mlp *mlp, const float *x, const float *t, int64_t B, float *grad, float *loss);
+/* `steps` full-batch Adam updates (each one replay of a captured CUDA graph). */
+int dr_mlp_train(dr_mlp *mlp, const float *x, const float *t, int64_t B, int steps, float lr,
+                 float *final_loss);
+int dr_tuner_features(int64_t X, uint64_t hbm_budget, int sm_count, int batch, float *out4);
+int dr_tuner_params(int64_t X, const float *y_normalised, dr_params *out);
+/* Proposal for X: inference on the device, mapped to parameters, then the
+ * endpoint-coverage and budget check; a failing proposal is replaced by the
+ * reference's default heuristic and *fallback is set to 1. */
+int dr_tuner_propose(dr_mlp *mlp, int64_t X, uint64_t hbm_budget, int sm_count, int batch,
+                     dr_params *out, int *fallback);
+
 /* Tables (reference: CompressedMertensTable / SieveTable) -------------------- */
 int dr_table_build(dr_ctx *ctx, int64_t u_total, int64_t u_dense, int64_t mu_limit,
                    const dr_params *tuning /* nullable: segment / block shape */,
