@@ -113,7 +113,8 @@ def dist_setup():
         import torch.distributed as dist
 
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        backend = os.environ.get("DR_DIST_BACKEND", "nccl")
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return world, rank, local
 
 
@@ -125,12 +126,14 @@ def barrier(world):
 
 
 def max_over_ranks(v, world):
+    """Max of a per-rank time over all ranks (NCCL on GPUs, gloo on CPU)."""
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -279,6 +282,23 @@ def run_engine(args, world, rank, local):
     check(eng.mertens(X, default).M)
     dsec, dhost, dstats = timed(default, max(1, args.steps // 2))
 
+    # the learned tuner's proposal (committed weights), same run
+    learned = None
+    wpath = os.path.join(ROOT, "deleglise-rivat_b200", "dr_b200", "tuner_weights.json")
+    if os.path.exists(wpath):
+        import numpy as np
+
+        mlp = dr_b200.MLP(eng)
+        with open(wpath) as f:
+            mlp.set_weights(np.array(json.load(f)["weights"], dtype=np.float32))
+        _, hbm = dr_b200.device_info(local)
+        lp, fb = mlp.propose(X, int(hbm * 0.9), 148, 1)
+        check(eng.mertens(X, lp).M)
+        lsec, _, _ = timed(lp, max(1, args.steps // 2))
+        learned = {"ms_per_step": lsec * 1e3, "u_total": lp.u_total, "cx": lp.cx, "segment_log2": lp.segment_log2,
+                   "fallback": fb, "speedup_vs_default": dsec / lsec}
+        mlp.close()
+
     tab = statistics.mean(s.table_ms for s in stats)
     plan = statistics.mean(s.plan_ms for s in stats)
     sums = statistics.mean(s.sums_ms for s in stats)
@@ -334,6 +354,10 @@ def run_engine(args, world, rank, local):
     # issue, not HBM: ops_per_s is the figure it is optimised on.
     alg = 2 * s0_.s1_ops + 0.5 * s0_.s2_ops
     achieved = alg / (sums / 1e3) / 1e9
+    # DRAM traffic: ncu dram__bytes_read.sum + dram__bytes_write.sum of sums_kernel
+    # measured at M(10^15) (profiles/sums_kernel_m1e15.md): 21.09 GB for 1.063e10
+    # ops = 1.98 B per op, scaled by this launch's op count (an estimate).
+    traffic = 1.98 * (s0_.s1_ops + s0_.s2_ops)
     line = {
         "metric": "sec per M(10^16)" if X == X_HEADLINE else f"sec per M({X})", "value": value, "unit": "s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_per * 1e3,
@@ -346,11 +370,14 @@ def run_engine(args, world, rank, local):
         "phases_ms": phases,
         "default_params": {"ms_per_step": dsec * 1e3, "u_total": default.u_total, "cx": default.cx,
                            "tuned_speedup": dsec / sec_per, "e2e_s": dhost},
+        "learned_tuner": learned,
         "gpu_launches": launches,
         "e2e": {"value": host_per / world, "unit": "s", "h2d_bytes_per_step": int(s0_.h2d_bytes),
                 "d2h_bytes_per_step": int(s0_.d2h_bytes)},
         "roofline": {"bound": "hbm", "kernel": "sums_kernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                     "traffic_basis": "ncu DRAM bytes per op at M(10^15), scaled by op count",
+                     "ops": {"s1_lookups": s0_.s1_ops, "s2_positions": s0_.s2_ops},
                      "note": "integer-issue bound (exact quotients + gathers); S1 lookups + S2 positions per second",
                      "ops_per_s": (s0_.s1_ops + s0_.s2_ops) / (sums / 1e3)},
         "clocks": clocks.summary(),

@@ -724,16 +724,27 @@ uint64_t dr_table_bytes(int64_t u_total, int64_t u_dense, int64_t mu_limit) {
     return (uint64_t)u_dense * 2 + (uint64_t)nwords * 20 + (uint64_t)(mu_limit / 192 + 2) * 16 + (uint64_t)nseg * 8;
 }
 
+uint64_t dr_query_bytes(int64_t X, const dr_params* p) {
+    if (!p || X < 1) return 0;
+    uint64_t b = dr_table_bytes(p->u_total, p->u_dense, p->mu_limit);
+    if (X > p->u_total && p->cx > 0.0) {
+        const double inv = 1.4143 * std::sqrt((double)X) / p->cx + 65.0;  // S1 reciprocals
+        const int64_t slots = 2 * num_candidates(X / p->u_total);        // ops + prefix
+        b += (uint64_t)(8.0 * inv) + (uint64_t)(p->mu_limit / 6 + 1) * 16 + (uint64_t)slots * 16 +
+             scan_u64_tmp_elems((u64)slots) * 8;
+    }
+    return b;
+}
+
 int dr_check_params(int64_t X, const dr_params* p, uint64_t hbm_budget) {
     if (!p) return fail(DR_ERR_ARG, "params is NULL");
     if (X < 1) return DR_OK;
     int rc = check_table_limits(p->u_total, p->u_dense, p->mu_limit);
     if (rc) return rc;
     if ((rc = check_query(X, *p, p->u_total, p->mu_limit))) return rc;
-    if (hbm_budget && dr_table_bytes(p->u_total, p->u_dense, p->mu_limit) > hbm_budget)
-        return fail(DR_ERR_NOMEM, "table needs %llu bytes, budget %llu",
-                    (unsigned long long)dr_table_bytes(p->u_total, p->u_dense, p->mu_limit),
-                    (unsigned long long)hbm_budget);
+    if (hbm_budget && dr_query_bytes(X, p) > hbm_budget)
+        return fail(DR_ERR_NOMEM, "query needs %llu device bytes, budget %llu",
+                    (unsigned long long)dr_query_bytes(X, p), (unsigned long long)hbm_budget);
     return DR_OK;
 }
 

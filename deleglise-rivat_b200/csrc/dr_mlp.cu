@@ -394,9 +394,27 @@ int dr_tuner_features(int64_t X, uint64_t hbm_budget, int sm_count, int batch, f
     return DR_OK;
 }
 
+// Shrink u (keeping cx, the dense tier and the endpoints) until the query's
+// device footprint fits 90% of the budget: the budget is a hard constraint of
+// the proposal, not a reason to discard it.
+static void project_to_budget(int64_t X, uint64_t budget, dr_params* p) {
+    if (!budget) return;
+    for (int it = 0; it < 64 && dr_query_bytes(X, p) > budget / 10 * 9; ++it) {
+        const int64_t S = isqrt_i64(X);
+        const int64_t endpoint = (int64_t)(p->cx * std::sqrt((double)X)) + 1000;
+        const int64_t floor_u = std::max(S + 1000, std::max(endpoint, p->u_dense));
+        int64_t u = std::max(floor_u, (int64_t)((double)p->u_total * 0.9));
+        u = ((u + 255) / 256) * 256;
+        if (u >= p->u_total) break;
+        p->u_total = u;
+        p->mu_limit = std::min(u, std::max(endpoint, X / u + 1000));
+    }
+}
+
 // The learned tuner's proposal for X: network inference on the device, mapped
-// to parameters, then the endpoint-coverage / budget check; a proposal that
-// fails it is replaced by the reference's default heuristic (*fallback = 1).
+// to parameters and projected onto the device budget, then the endpoint-
+// coverage check; a proposal that fails it is replaced by the reference's
+// default heuristic (*fallback = 1).
 int dr_tuner_propose(dr_mlp* n, int64_t X, uint64_t hbm_budget, int sm_count, int batch, dr_params* out,
                      int* fallback) {
     if (!n || !out) return mlp_fail(DR_ERR_ARG, "dr_tuner_propose: bad argument");
@@ -405,6 +423,7 @@ int dr_tuner_propose(dr_mlp* n, int64_t X, uint64_t hbm_budget, int sm_count, in
     int rc = dr_mlp_forward(n, f, 1, y);
     if (rc) return rc;
     outputs_to_params(X, y, out);
+    if (X > 0) project_to_budget(X, hbm_budget, out);
     int fb = 0;
     if (X < 1 || dr_check_params(X, out, hbm_budget) != DR_OK) {
         fb = 1;

@@ -126,6 +126,7 @@ def lib():
             "dr_default_params": (i32, [i64, i32, P]),
             "dr_check_params": (i32, [i64, P, u64]),
             "dr_table_bytes": (u64, [i64, i64, i64]),
+            "dr_query_bytes": (u64, [i64, P]),
             "dr_mertens": (i32, [vp, i64, P, ctypes.POINTER(i64), S]),
             "dr_mertens_batch": (i32, [vp, ctypes.POINTER(i64), i64, P, ctypes.POINTER(i64), S]),
             "dr_batch_checksums": (i32, [vp, ctypes.POINTER(u64), i64]),
@@ -165,7 +166,7 @@ def exported_symbols() -> list:
     lib()
     return [
         "dr_ctx_create", "dr_ctx_destroy", "dr_last_error", "dr_ctx_set_hbm_budget", "dr_device_info",
-        "dr_default_params", "dr_check_params", "dr_table_bytes", "dr_mertens", "dr_mertens_batch",
+        "dr_default_params", "dr_check_params", "dr_table_bytes", "dr_query_bytes", "dr_mertens", "dr_mertens_batch",
         "dr_batch_checksums", "dr_table_build", "dr_table_read", "dr_table_read_wheel", "dr_table_checksums",
         "dr_debug_udiv", "dr_debug_piece", "dr_table_build_noalloc", "dr_autotune_batch",
         "dr_mlp_create", "dr_mlp_destroy", "dr_mlp_num_params", "dr_mlp_set_weights", "dr_mlp_get_weights",
@@ -192,6 +193,11 @@ def check_params(X: int, p: Params, budget: int = 0) -> int:
 
 def table_bytes(u_total: int, u_dense: int, mu_limit: int) -> int:
     return int(lib().dr_table_bytes(int(u_total), int(u_dense), int(mu_limit)))
+
+
+def query_bytes(X: int, p: Params) -> int:
+    """Device bytes one query needs (table + reciprocal tables + work arrays)."""
+    return int(lib().dr_query_bytes(int(X), ctypes.byref(p)))
 
 
 def choose_cx(X: int) -> float:

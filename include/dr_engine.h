@@ -98,6 +98,9 @@ int dr_default_params(int64_t X, int policy, dr_params *out);
 int dr_check_params(int64_t X, const dr_params *p, uint64_t hbm_budget);
 /* Device bytes a table with these limits needs. */
 uint64_t dr_table_bytes(int64_t u_total, int64_t u_dense, int64_t mu_limit);
+/* Device bytes one query needs: the table plus its reciprocal tables and
+ * work arrays (what dr_check_params compares with the budget). */
+uint64_t dr_query_bytes(int64_t X, const dr_params *p);
 
 /* Single query (reference: compute_mertens / compute_compressed) ------------- */
 int dr_mertens(dr_ctx *ctx, int64_t X, const dr_params *p /* NULL: reference policy */,
