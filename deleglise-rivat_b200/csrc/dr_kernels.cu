@@ -520,14 +520,28 @@ void launch_scan_u64(const u64* in, u64* out, u64 n, u64* tmp, size_t, cudaStrea
 // Persistent S1 / S2 kernel over the flattened op space.
 // ---------------------------------------------------------------------------
 
-constexpr int kS1Unroll = 4;  // independent gathers in flight per lane
+// Code-shape knobs of the sums kernel (chosen by measurement on B200).
+#ifndef DRB_S1_INLINE
+#define DRB_S1_INLINE __device__ __forceinline__
+#endif
+#ifndef DRB_S2_INLINE
+#define DRB_S2_INLINE __device__ __forceinline__
+#endif
+#ifndef DRB_SUMS_MINB
+#define DRB_SUMS_MINB 1
+#endif
+#ifndef DRB_S1_UNROLL
+#define DRB_S1_UNROLL 8
+#endif
+
+constexpr int kS1Unroll = DRB_S1_UNROLL;  // independent gathers in flight per lane
 constexpr int kS2Unroll = 2;
 
 // sum of M(floor(y/n)) over n = n0 + stride*i, i in [i0, i1), lanes interleaved.
 // Groups of kS1Unroll iterations issue their reciprocal loads, quotients and
 // table gathers back to back; a group whose divisors are all tabulated and
 // whose quotients all fall in the dense tier takes the branch-free path.
-__device__ __forceinline__ i64 s1_part(const SumsArgs& a, u64 y, i64 n0, int stride, u64 i0, u64 i1, int lane) {
+DRB_S1_INLINE i64 s1_part(const SumsArgs& a, u64 y, i64 n0, int stride, u64 i0, u64 i1, int lane) {
     i64 acc = 0;
     const u64 lim = (u64)a.inv_limit;
     const u64 ud = (u64)a.T.u_dense;
@@ -567,29 +581,60 @@ __device__ __forceinline__ i64 s1_part(const SumsArgs& a, u64 y, i64 n0, int str
     return acc;
 }
 
-// mu(j) * piece(floor(y/j)) for one wheel position m (j = 6m+1, 6m+5 within [jlo, jhi])
-__device__ __forceinline__ u64 s2_position(const SumsArgs& a, u64 y, const PieceCoef& pc, i64 jlo, i64 jhi, u64 m,
+// Summand kinds: most positions fall in pieces whose summand needs no
+// division by 12 (the split of f_A(q) - f_B(q/2) and f_A(q) of dr_device.cuh):
+//   kind 1: q            (pieces 8, 12)
+//   kind 2: (q + 1) >> 1 (pieces 7, 11)
+//   kind 3: q & 1        (piece 6)
+//   kind 4: (q >> 2) + (q & 1)  (piece 5)
+//   kind 0: a * (q / 12) + T[q mod 12]  (pieces 1-4, 9, 10)
+__host__ __device__ constexpr int piece_kind(int piece) {
+    return piece == 8 || piece == 12 ? 1 : piece == 7 || piece == 11 ? 2 : piece == 6 ? 3 : piece == 5 ? 4 : 0;
+}
+
+template <int KIND>
+__device__ __forceinline__ i64 piece_value(const PieceCoef& pc, u64 q) {
+    if (KIND == 1) return (i64)q;
+    if (KIND == 2) return (i64)((q + 1) >> 1);
+    if (KIND == 3) return (i64)(q & 1);
+    if (KIND == 4) return (i64)((q >> 2) + (q & 1));
+    return piece_eval(pc, q);
+}
+
+// mu(j) * piece(floor(y/j)) for one wheel position m (j = 6m+1, 6m+5); only the
+// first and last position of a piece can have a j outside [jlo, jhi].
+template <int KIND>
+__device__ __forceinline__ u64 s2_position(u64 y, const PieceCoef& pc, i64 jlo, i64 jhi, u64 m, bool edge,
                                            const uint4 w, const ulonglong2 iv) {
     const uint32_t b = (uint32_t)(m & 31u);
-    const i64 j1 = (i64)(6 * m + 1), j5 = (i64)(6 * m + 5);
-    u64 acc = 0;
-    if (((w.x >> b) & 1u) && j1 >= jlo && j1 <= jhi) {
-        const i64 v = piece_eval(pc, udiv_inv(y, (u64)j1, iv.x));
-        acc += ((w.y >> b) & 1u) ? (u64)(-v) : (u64)v;
+    bool t1 = (w.x >> b) & 1u, t5 = (w.z >> b) & 1u;
+    if (edge) {
+        const i64 j1 = (i64)(6 * m + 1), j5 = (i64)(6 * m + 5);
+        t1 = t1 && j1 >= jlo && j1 <= jhi;
+        t5 = t5 && j5 >= jlo && j5 <= jhi;
     }
-    if (((w.z >> b) & 1u) && j5 >= jlo && j5 <= jhi) {
-        const i64 v = piece_eval(pc, udiv_inv(y, (u64)j5, iv.y));
-        acc += ((w.w >> b) & 1u) ? (u64)(-v) : (u64)v;
+    u64 acc = 0;
+    if (t1) {
+        const u64 v = (u64)piece_value<KIND>(pc, udiv_inv(y, 6 * m + 1, iv.x));
+        const u64 sg = 0ull - (u64)((w.y >> b) & 1u);  // all ones when mu = -1
+        acc += (v ^ sg) - sg;
+    }
+    if (t5) {
+        const u64 v = (u64)piece_value<KIND>(pc, udiv_inv(y, 6 * m + 5, iv.y));
+        const u64 sg = 0ull - (u64)((w.w >> b) & 1u);
+        acc += (v ^ sg) - sg;
     }
     return acc;
 }
 
 // sum of mu(j) * piece(floor(y/j)) for j in {6m+1, 6m+5} within [jlo, jhi],
-// m = jlo/6 + i, i in [i0, i1)
-__device__ __forceinline__ u64 s2_part(const SumsArgs& a, u64 y, const PieceCoef pc, i64 jlo, i64 jhi, u64 i0,
-                                       u64 i1, int lane) {
+// m = jlo/6 + i, i in [i0, i1) of the piece's mcnt positions
+template <int KIND>
+__device__ __forceinline__ u64 s2_part(const SumsArgs& a, u64 y, const PieceCoef pc, i64 jlo, i64 jhi, u64 mcnt,
+                                       u64 i0, u64 i1, int lane) {
     u64 acc = 0;
     const u64 m0 = (u64)(jlo / 6);
+    const u64 last = mcnt - 1;
     u64 i = i0 + lane;
     for (; i + 32 * (kS2Unroll - 1) < i1; i += 32 * kS2Unroll) {
         uint4 w[kS2Unroll];
@@ -601,13 +646,29 @@ __device__ __forceinline__ u64 s2_part(const SumsArgs& a, u64 y, const PieceCoef
             iv[k] = __ldg(a.invw + m);
         }
 #pragma unroll
-        for (int k = 0; k < kS2Unroll; ++k) acc += s2_position(a, y, pc, jlo, jhi, m0 + i + 32 * k, w[k], iv[k]);
+        for (int k = 0; k < kS2Unroll; ++k) {
+            const u64 ii = i + 32 * k;
+            acc += s2_position<KIND>(y, pc, jlo, jhi, m0 + ii, ii == 0 || ii == last, w[k], iv[k]);
+        }
     }
     for (; i < i1; i += 32) {
         const u64 m = m0 + i;
-        acc += s2_position(a, y, pc, jlo, jhi, m, __ldg(a.T.wheel + (m >> 5)), __ldg(a.invw + m));
+        acc += s2_position<KIND>(y, pc, jlo, jhi, m, i == 0 || i == last, __ldg(a.T.wheel + (m >> 5)),
+                                 __ldg(a.invw + m));
     }
     return acc;
+}
+
+DRB_S2_INLINE u64 s2_dispatch(const SumsArgs& a, u64 y, int piece, i64 jlo, i64 jhi, u64 mcnt, u64 i0,
+                                        u64 i1, int lane) {
+    const PieceCoef pc = c_piece[piece];
+    switch (piece_kind(piece)) {
+    case 1: return s2_part<1>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
+    case 2: return s2_part<2>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
+    case 3: return s2_part<3>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
+    case 4: return s2_part<4>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
+    default: return s2_part<0>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
+    }
 }
 
 __device__ __forceinline__ u64 upper_slot(const u64* prefix, u64 n_slots, u64 o) {
@@ -621,7 +682,7 @@ __device__ __forceinline__ u64 upper_slot(const u64* prefix, u64 n_slots, u64 o)
     return lo;
 }
 
-__global__ void __launch_bounds__(256) sums_kernel(const SumsArgs a) {
+__global__ void __launch_bounds__(256, DRB_SUMS_MINB) sums_kernel(const SumsArgs a) {
     __shared__ EvalDesc sdesc[8];  // one decoded evaluation per warp
     const int lane = threadIdx.x & 31;
     EvalDesc& d = sdesc[threadIdx.x >> 5];
@@ -690,7 +751,8 @@ __global__ void __launch_bounds__(256) sums_kernel(const SumsArgs a) {
                     s1 += sg > 0 ? (u64)part : (u64)(-part);
                 } else {
                     const int p = g - 2;
-                    const u64 part = s2_part(a, y, c_piece[d.piece0 + p], d.jlo[p], d.jhi[p], a0 - sb, a1 - sb, lane);
+                    const u64 part = s2_dispatch(a, y, d.piece0 + p, d.jlo[p], d.jhi[p], (u64)d.mcnt[p], a0 - sb,
+                                                 a1 - sb, lane);
                     s2 += coef > 0 ? part : (u64)(0 - part);
                 }
             }

@@ -19,7 +19,7 @@ from dataclasses import dataclass
 from typing import Iterable, Optional, Sequence
 
 _PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-_LIB_PATH = os.path.join(_PKG_DIR, "lib", "libdrb200.so")
+_LIB_PATH = os.environ.get("DR_B200_LIB") or os.path.join(_PKG_DIR, "lib", "libdrb200.so")
 _CSRC = os.path.join(_PKG_DIR, "csrc")
 
 DR_OK = 0
