@@ -47,13 +47,17 @@ __device__ __forceinline__ u64 udiv_u64_u32(u64 y, uint32_t d, float inv) {
     return q;
 }
 
-// floor(y / n) from a tabulated reciprocal inv = floor((2^64 - 1) / n), n >= 1.
-// q' = umulhi(y, inv) satisfies y/n - 2 < q' <= floor(y/n) (inv undershoots
-// 2^64/n by less than 1 + 1/n), so one integer correction makes it exact.
-__device__ __forceinline__ u64 udiv_inv(u64 y, u64 n, u64 inv) {
-    const u64 q = __umul64hi(y, inv);
-    const u64 r = y - q * n;
-    return q + (r >= n ? 1ull : 0ull);
+// floor(y / n) from a tabulated double reciprocal r = RN(1/n), for n < 2^32 and
+// y / n < 2^50, with yd = RN(y).  p = RN(yd * r) is within (y/n) * 3 * 2^-53 < 3/8
+// of y/n, so trunc(p) is floor(y/n) or a neighbour of it; the exact remainder
+// y - trunc(p) * n, which lies in [-n, 2n), selects the right one.  trunc(p) is
+// the low mantissa of RZ(p + 2^52) (0 <= p < 2^52, where that sum has ulp 1).
+__device__ __forceinline__ u64 udiv_rcp(u64 y, double yd, uint32_t n, double r) {
+    const double p = __dmul_rn(yd, r);
+    const u64 qe = (u64)__double_as_longlong(__dadd_rz(p, 4503599627370496.0)) & 0xFFFFFFFFFFFFFull;
+    const u64 prod = (u64)(uint32_t)qe * n + ((u64)((uint32_t)(qe >> 32) * n) << 32);  // qe * n < 2^64
+    const i64 rem = (i64)(y - prod);
+    return qe + (u64)(i64)((int)(rem >= (i64)n) - (int)(rem < 0));
 }
 
 __device__ __forceinline__ u64 udiv(u64 y, u64 d) {

@@ -464,7 +464,7 @@ int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq,
     launch_direct((const QueryDev*)c->queries.p, qn, T, (u64*)c->acc.p, c->stream);
     int launches = 1;
     if (slots > 0) {
-        launch_inverse((u64*)c->inv.p, inv_limit, (ulonglong2*)c->invw.p, invw_count, c->sm_count, c->stream);
+        launch_inverse((double*)c->inv.p, inv_limit, (double2*)c->invw.p, invw_count, c->sm_count, c->stream);
         launch_plan((const QueryDev*)c->queries.p, qn, T, slots, (u64*)c->ops.p, (u64*)c->acc.p, (i64*)c->counts.p,
                     c->sm_count, c->stream);
         launch_scan_u64((const u64*)c->ops.p, (u64*)c->prefix.p, slots, (u64*)c->scan_tmp.p,
@@ -483,9 +483,9 @@ int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq,
         sa.ticket = (u64*)c->ticket.p;
         sa.acc = (u64*)c->acc.p;
         sa.chunk_log2 = tuning ? tuning->chunk_log2 : 0;
-        sa.inv = (const u64*)c->inv.p;
+        sa.rcp = (const double*)c->inv.p;
         sa.inv_limit = inv_limit;
-        sa.invw = (const ulonglong2*)c->invw.p;
+        sa.invw = (const double2*)c->invw.p;
         sa.invw_count = invw_count;
         int per_sm = 0;
         sums_kernel_occupancy(256, &per_sm);
@@ -1012,7 +1012,7 @@ int dr_table_checksums(dr_ctx* c, dr_table_sums* out) {
     return DR_OK;
 }
 
-int dr_debug_udiv(dr_ctx* c, const uint64_t* y, const uint64_t* d, int64_t n, uint64_t* q) {
+static int debug_udiv(dr_ctx* c, const uint64_t* y, const uint64_t* d, int64_t n, uint64_t* q, int rcp) {
     if (!c || !y || !d || !q || n < 0) return fail(DR_ERR_ARG, "bad argument");
     if (n == 0) return DR_OK;
     CU(cudaSetDevice(c->device));
@@ -1023,11 +1023,19 @@ int dr_debug_udiv(dr_ctx* c, const uint64_t* y, const uint64_t* d, int64_t n, ui
     u64* dq = dd + n;
     CU(cudaMemcpyAsync(dy, y, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream));
     CU(cudaMemcpyAsync(dd, d, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream));
-    launch_debug_udiv(dy, dd, dq, n, c->stream);
+    launch_debug_udiv(dy, dd, dq, n, rcp, c->stream);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(q, dq, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
     CU(cudaStreamSynchronize(c->stream));
     return DR_OK;
+}
+
+int dr_debug_udiv(dr_ctx* c, const uint64_t* y, const uint64_t* d, int64_t n, uint64_t* q) {
+    return debug_udiv(c, y, d, n, q, 0);
+}
+
+int dr_debug_udiv_rcp(dr_ctx* c, const uint64_t* y, const uint64_t* d, int64_t n, uint64_t* q) {
+    return debug_udiv(c, y, d, n, q, 1);
 }
 
 int dr_debug_piece(dr_ctx* c, const int32_t* piece, const uint64_t* q, int64_t n, int64_t* out) {

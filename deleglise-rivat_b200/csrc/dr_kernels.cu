@@ -80,7 +80,8 @@ __device__ int block_excl_scan(int32_t* a, int n, int32_t* wtot) {
     return total;
 }
 
-// y mod d from a tabulated reciprocal inv = floor((2^64-1)/d) (see udiv_inv)
+// y mod d from a tabulated reciprocal inv = floor((2^64-1)/d): umulhi(y, inv)
+// undershoots floor(y/d) by at most one, so one subtraction corrects the remainder
 __device__ __forceinline__ u64 umod_inv(u64 y, u64 d, u64 inv) {
     const u64 r = y - __umul64hi(y, inv) * d;
     return r >= d ? r - d : r;
@@ -542,20 +543,24 @@ constexpr int kS2Unroll = 2;
 // table gathers back to back; a group whose divisors are all tabulated and
 // whose quotients all fall in the dense tier takes the branch-free path.
 DRB_S1_INLINE i64 s1_part(const SumsArgs& a, u64 y, i64 n0, int stride, u64 i0, u64 i1, int lane) {
+    // every q = floor(y/n) here is at most u_total < 2^42, so the reciprocal
+    // estimate (udiv_rcp) applies to every tabulated n
     i64 acc = 0;
     const u64 lim = (u64)a.inv_limit;
     const u64 ud = (u64)a.T.u_dense;
     const u64 nstep = 32ull * (u64)stride;
+    const double yd = __ull2double_rn(y);
     u64 i = i0 + lane;
     for (; i + 32 * (kS1Unroll - 1) < i1; i += 32 * kS1Unroll) {
         const u64 nfirst = (u64)n0 + (u64)stride * i;
         const u64 nlast = nfirst + nstep * (kS1Unroll - 1);
         if (nlast <= lim) {
-            u64 iv[kS1Unroll], q[kS1Unroll];
+            double rv[kS1Unroll];
+            u64 q[kS1Unroll];
 #pragma unroll
-            for (int k = 0; k < kS1Unroll; ++k) iv[k] = __ldg(a.inv + nfirst + nstep * k);
+            for (int k = 0; k < kS1Unroll; ++k) rv[k] = __ldg(a.rcp + nfirst + nstep * k);
 #pragma unroll
-            for (int k = 0; k < kS1Unroll; ++k) q[k] = udiv_inv(y, nfirst + nstep * k, iv[k]);
+            for (int k = 0; k < kS1Unroll; ++k) q[k] = udiv_rcp(y, yd, (uint32_t)(nfirst + nstep * k), rv[k]);
             if (q[0] <= ud && q[kS1Unroll - 1] >= 1) {  // q falls with n: all in the dense tier
                 int32_t m[kS1Unroll];
 #pragma unroll
@@ -570,13 +575,13 @@ DRB_S1_INLINE i64 s1_part(const SumsArgs& a, u64 y, i64 n0, int stride, u64 i0, 
 #pragma unroll
             for (int k = 0; k < kS1Unroll; ++k) {
                 const u64 n = nfirst + nstep * k;
-                acc += table_M(a.T, n <= lim ? udiv_inv(y, n, __ldg(a.inv + n)) : udiv(y, n));
+                acc += table_M(a.T, n <= lim ? udiv_rcp(y, yd, (uint32_t)n, __ldg(a.rcp + n)) : udiv(y, n));
             }
         }
     }
     for (; i < i1; i += 32) {
         const u64 n = (u64)n0 + (u64)stride * i;
-        acc += table_M(a.T, n <= lim ? udiv_inv(y, n, __ldg(a.inv + n)) : udiv(y, n));
+        acc += table_M(a.T, n <= lim ? udiv_rcp(y, yd, (uint32_t)n, __ldg(a.rcp + n)) : udiv(y, n));
     }
     return acc;
 }
@@ -603,9 +608,9 @@ __device__ __forceinline__ i64 piece_value(const PieceCoef& pc, u64 q) {
 
 // mu(j) * piece(floor(y/j)) for one wheel position m (j = 6m+1, 6m+5); only the
 // first and last position of a piece can have a j outside [jlo, jhi].
-template <int KIND>
-__device__ __forceinline__ u64 s2_position(u64 y, const PieceCoef& pc, i64 jlo, i64 jhi, u64 m, bool edge,
-                                           const uint4 w, const ulonglong2 iv) {
+template <int KIND, bool RCP>
+__device__ __forceinline__ u64 s2_position(u64 y, double yd, const PieceCoef& pc, i64 jlo, i64 jhi, u64 m,
+                                           bool edge, const uint4 w, const double2 iv) {
     const uint32_t b = (uint32_t)(m & 31u);
     bool t1 = (w.x >> b) & 1u, t5 = (w.z >> b) & 1u;
     if (edge) {
@@ -615,12 +620,14 @@ __device__ __forceinline__ u64 s2_position(u64 y, const PieceCoef& pc, i64 jlo, 
     }
     u64 acc = 0;
     if (t1) {
-        const u64 v = (u64)piece_value<KIND>(pc, udiv_inv(y, 6 * m + 1, iv.x));
+        const u64 q = RCP ? udiv_rcp(y, yd, (uint32_t)(6 * m + 1), iv.x) : udiv(y, 6 * m + 1);
+        const u64 v = (u64)piece_value<KIND>(pc, q);
         const u64 sg = 0ull - (u64)((w.y >> b) & 1u);  // all ones when mu = -1
         acc += (v ^ sg) - sg;
     }
     if (t5) {
-        const u64 v = (u64)piece_value<KIND>(pc, udiv_inv(y, 6 * m + 5, iv.y));
+        const u64 q = RCP ? udiv_rcp(y, yd, (uint32_t)(6 * m + 5), iv.y) : udiv(y, 6 * m + 5);
+        const u64 v = (u64)piece_value<KIND>(pc, q);
         const u64 sg = 0ull - (u64)((w.w >> b) & 1u);
         acc += (v ^ sg) - sg;
     }
@@ -628,17 +635,19 @@ __device__ __forceinline__ u64 s2_position(u64 y, const PieceCoef& pc, i64 jlo, 
 }
 
 // sum of mu(j) * piece(floor(y/j)) for j in {6m+1, 6m+5} within [jlo, jhi],
-// m = jlo/6 + i, i in [i0, i1) of the piece's mcnt positions
-template <int KIND>
+// m = jlo/6 + i, i in [i0, i1) of the piece's mcnt positions.  RCP: every j of
+// the range is below 2^32 and every y/j below 2^50 (udiv_rcp applies).
+template <int KIND, bool RCP>
 __device__ __forceinline__ u64 s2_part(const SumsArgs& a, u64 y, const PieceCoef pc, i64 jlo, i64 jhi, u64 mcnt,
                                        u64 i0, u64 i1, int lane) {
     u64 acc = 0;
+    const double yd = __ull2double_rn(y);
     const u64 m0 = (u64)(jlo / 6);
     const u64 last = mcnt - 1;
     u64 i = i0 + lane;
     for (; i + 32 * (kS2Unroll - 1) < i1; i += 32 * kS2Unroll) {
         uint4 w[kS2Unroll];
-        ulonglong2 iv[kS2Unroll];
+        double2 iv[kS2Unroll];
 #pragma unroll
         for (int k = 0; k < kS2Unroll; ++k) {
             const u64 m = m0 + i + 32 * k;
@@ -648,12 +657,12 @@ __device__ __forceinline__ u64 s2_part(const SumsArgs& a, u64 y, const PieceCoef
 #pragma unroll
         for (int k = 0; k < kS2Unroll; ++k) {
             const u64 ii = i + 32 * k;
-            acc += s2_position<KIND>(y, pc, jlo, jhi, m0 + ii, ii == 0 || ii == last, w[k], iv[k]);
+            acc += s2_position<KIND, RCP>(y, yd, pc, jlo, jhi, m0 + ii, ii == 0 || ii == last, w[k], iv[k]);
         }
     }
     for (; i < i1; i += 32) {
         const u64 m = m0 + i;
-        acc += s2_position<KIND>(y, pc, jlo, jhi, m, i == 0 || i == last, __ldg(a.T.wheel + (m >> 5)),
+        acc += s2_position<KIND, RCP>(y, yd, pc, jlo, jhi, m, i == 0 || i == last, __ldg(a.T.wheel + (m >> 5)),
                                  __ldg(a.invw + m));
     }
     return acc;
@@ -662,12 +671,15 @@ __device__ __forceinline__ u64 s2_part(const SumsArgs& a, u64 y, const PieceCoef
 DRB_S2_INLINE u64 s2_dispatch(const SumsArgs& a, u64 y, int piece, i64 jlo, i64 jhi, u64 mcnt, u64 i0,
                                         u64 i1, int lane) {
     const PieceCoef pc = c_piece[piece];
+    const u64 m0 = (u64)(jlo / 6);
+    const u64 jmin = 6 * (m0 + i0) + 1, jmax = 6 * (m0 + i1) + 5;  // bounds every j of [i0, i1)
+    if (jmax >> 32 || (y >> 50) >= jmin) return s2_part<0, false>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
     switch (piece_kind(piece)) {
-    case 1: return s2_part<1>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
-    case 2: return s2_part<2>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
-    case 3: return s2_part<3>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
-    case 4: return s2_part<4>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
-    default: return s2_part<0>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
+    case 1: return s2_part<1, true>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
+    case 2: return s2_part<2, true>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
+    case 3: return s2_part<3, true>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
+    case 4: return s2_part<4, true>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
+    default: return s2_part<0, true>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
     }
 }
 
@@ -769,19 +781,19 @@ __global__ void __launch_bounds__(256, DRB_SUMS_MINB) sums_kernel(const SumsArgs
     }
 }
 
-// inv[n] = floor((2^64-1)/n) for 1 <= n <= inv_limit; invw[m] = {inv(6m+1), inv(6m+5)}.
-__global__ void inverse_kernel(u64* inv, i64 inv_limit, ulonglong2* invw, i64 invw_count) {
+// rcp[n] = RN(1/n) for 1 <= n <= inv_limit; invw[m] = {rcp(6m+1), rcp(6m+5)}.
+__global__ void inverse_kernel(double* rcp, i64 inv_limit, double2* invw, i64 invw_count) {
     const i64 stride = (i64)gridDim.x * blockDim.x;
     const i64 t0 = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    for (i64 n = t0; n <= inv_limit; n += stride) inv[n] = n ? udiv(~0ull, (u64)n) : 0ull;
+    for (i64 n = t0; n <= inv_limit; n += stride) rcp[n] = n ? __drcp_rn((double)n) : 0.0;
     for (i64 m = t0; m < invw_count; m += stride)
-        invw[m] = make_ulonglong2(udiv(~0ull, (u64)(6 * m + 1)), udiv(~0ull, (u64)(6 * m + 5)));
+        invw[m] = make_double2(__drcp_rn((double)(6 * m + 1)), __drcp_rn((double)(6 * m + 5)));
 }
 
-void launch_inverse(u64* inv, i64 inv_limit, ulonglong2* invw, i64 invw_count, int sm_count, cudaStream_t s) {
+void launch_inverse(double* rcp, i64 inv_limit, double2* invw, i64 invw_count, int sm_count, cudaStream_t s) {
     const i64 work = std::max<i64>(inv_limit + 1, invw_count);
     const int grid = (int)std::min<i64>((work + 255) / 256, (i64)sm_count * 16);
-    inverse_kernel<<<std::max(grid, 1), 256, 0, s>>>(inv, inv_limit, invw, invw_count);
+    inverse_kernel<<<std::max(grid, 1), 256, 0, s>>>(rcp, inv_limit, invw, invw_count);
 }
 
 void sums_kernel_occupancy(int block, int* per_sm) {
@@ -861,9 +873,15 @@ void launch_table_sums(const TableView& T, i64 nwords, u64* out6, int sm_count, 
 // ---------------------------------------------------------------------------
 // Test support: the device quotient and S2 summand on caller-chosen inputs.
 // ---------------------------------------------------------------------------
-__global__ void debug_udiv_kernel(const u64* y, const u64* d, u64* q, i64 n) {
+// rcp = 0: udiv; rcp = 1: udiv_rcp with a device-computed reciprocal, ~0 where
+// (y, d) is outside its domain (d >= 2^32 or y/d >= 2^50)
+__global__ void debug_udiv_kernel(const u64* y, const u64* d, u64* q, i64 n, int rcp) {
     const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) q[i] = d[i] ? udiv(y[i], d[i]) : 0;
+    if (i >= n) return;
+    const u64 yy = y[i], dd = d[i];
+    if (!rcp) q[i] = dd ? udiv(yy, dd) : 0;
+    else if (dd == 0 || (dd >> 32) || (yy >> 50) >= dd) q[i] = ~0ull;
+    else q[i] = udiv_rcp(yy, __ull2double_rn(yy), (uint32_t)dd, __drcp_rn((double)dd));
 }
 
 __global__ void debug_piece_kernel(const int32_t* piece, const u64* q, i64* out, i64 n) {
@@ -874,8 +892,8 @@ __global__ void debug_piece_kernel(const int32_t* piece, const u64* q, i64* out,
     }
 }
 
-void launch_debug_udiv(const u64* y, const u64* d, u64* q, i64 n, cudaStream_t s) {
-    if (n > 0) debug_udiv_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(y, d, q, n);
+void launch_debug_udiv(const u64* y, const u64* d, u64* q, i64 n, int rcp, cudaStream_t s) {
+    if (n > 0) debug_udiv_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(y, d, q, n, rcp);
 }
 
 void launch_debug_piece(const int32_t* piece, const u64* q, i64* out, i64 n, cudaStream_t s) {

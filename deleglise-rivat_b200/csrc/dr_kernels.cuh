@@ -42,9 +42,9 @@ struct SumsArgs {
     u64* ticket;        // [0]: work-queue counter, [1]: error flag; zeroed before launch
     u64* acc;           // [3 * nq]: C, S1, S2
     int chunk_log2;     // 0: chosen on the device from the total
-    const u64* inv;          // inv[n] = floor((2^64-1)/n), 1 <= n <= inv_limit
+    const double* rcp;       // rcp[n] = RN(1/n), 1 <= n <= inv_limit (< 2^32)
     i64 inv_limit;
-    const ulonglong2* invw;  // invw[m] = {inv(6m+1), inv(6m+5)}, m < invw_count
+    const double2* invw;     // invw[m] = {rcp(6m+1), rcp(6m+5)}, m < invw_count
     i64 invw_count;
 };
 
@@ -70,7 +70,7 @@ void launch_scan_u64(const u64* in, u64* out, u64 n, u64* tmp, size_t tmp_elems,
 size_t scan_u64_tmp_elems(u64 n);
 void launch_sums(const SumsArgs& a, int grid, int block, cudaStream_t s);
 // Reciprocal tables shared by every evaluation of a launch.
-void launch_inverse(u64* inv, i64 inv_limit, ulonglong2* invw, i64 invw_count, int sm_count, cudaStream_t s);
+void launch_inverse(double* rcp, i64 inv_limit, double2* invw, i64 invw_count, int sm_count, cudaStream_t s);
 void launch_direct(const QueryDev* q, int nq, const TableView& T, u64* acc, cudaStream_t s);
 void launch_table_read(const TableView& T, i64 first, i64 count, int32_t* M, int8_t* mu, int8_t* wheel_mu,
                        cudaStream_t s);
@@ -82,7 +82,7 @@ int record_error(int code, const char* msg);
 // how many CTAs of `block` threads fit on one SM.
 void sieve_kernel_attrs(size_t smem, int block, int* per_sm);
 void sums_kernel_occupancy(int block, int* per_sm);
-void launch_debug_udiv(const u64* y, const u64* d, u64* q, i64 n, cudaStream_t s);
+void launch_debug_udiv(const u64* y, const u64* d, u64* q, i64 n, int rcp, cudaStream_t s);
 void launch_debug_piece(const int32_t* piece, const u64* q, i64* out, i64 n, cudaStream_t s);
 
 }  // namespace drb

@@ -135,6 +135,7 @@ def lib():
             "dr_table_read_wheel": (i32, [vp, i64, i64, ctypes.POINTER(ctypes.c_int8)]),
             "dr_table_checksums": (i32, [vp, ctypes.POINTER(TableSums)]),
             "dr_debug_udiv": (i32, [vp, ctypes.POINTER(u64), ctypes.POINTER(u64), i64, ctypes.POINTER(u64)]),
+            "dr_debug_udiv_rcp": (i32, [vp, ctypes.POINTER(u64), ctypes.POINTER(u64), i64, ctypes.POINTER(u64)]),
             "dr_debug_piece": (i32, [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(u64), i64,
                                      ctypes.POINTER(i64)]),
             "dr_table_build_noalloc": (i32, [i32, vp, i64, i64, i64, vp, vp, vp, vp]),
@@ -168,7 +169,7 @@ def exported_symbols() -> list:
         "dr_ctx_create", "dr_ctx_destroy", "dr_last_error", "dr_ctx_set_hbm_budget", "dr_device_info",
         "dr_default_params", "dr_check_params", "dr_table_bytes", "dr_query_bytes", "dr_mertens", "dr_mertens_batch",
         "dr_batch_checksums", "dr_table_build", "dr_table_read", "dr_table_read_wheel", "dr_table_checksums",
-        "dr_debug_udiv", "dr_debug_piece", "dr_table_build_noalloc", "dr_autotune_batch",
+        "dr_debug_udiv", "dr_debug_udiv_rcp", "dr_debug_piece", "dr_table_build_noalloc", "dr_autotune_batch",
         "dr_mlp_create", "dr_mlp_destroy", "dr_mlp_num_params", "dr_mlp_set_weights", "dr_mlp_get_weights",
         "dr_mlp_forward", "dr_mlp_grad", "dr_mlp_train", "dr_tuner_features", "dr_tuner_params", "dr_tuner_propose",
     ]
@@ -305,13 +306,15 @@ class Engine:
         return mu
 
     # --- device arithmetic (test support) --------------------------------------
-    def debug_udiv(self, ys, ds):
-        """floor(y/d) computed by the device quotient routine."""
+    def debug_udiv(self, ys, ds, rcp: bool = False):
+        """floor(y/d) computed by the device quotient routine (rcp: the
+        reciprocal-estimate routine of the S1/S2 loops; 2^64-1 outside its domain)."""
         n = len(ys)
         Y = (ctypes.c_uint64 * n)(*[int(v) for v in ys])
         D = (ctypes.c_uint64 * n)(*[int(v) for v in ds])
         Q = (ctypes.c_uint64 * n)()
-        _check(lib().dr_debug_udiv(self._ctx, Y, D, n, Q))
+        fn = lib().dr_debug_udiv_rcp if rcp else lib().dr_debug_udiv
+        _check(fn(self._ctx, Y, D, n, Q))
         return list(Q)
 
     def debug_piece(self, pieces, qs):

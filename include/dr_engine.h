@@ -166,8 +166,11 @@ int dr_table_read_wheel(dr_ctx *ctx, int64_t first, int64_t count, int8_t *mu);
 /* Test support: the device's exact quotient floor(y[i]/d[i]) and S2 summand
  * piece[i](q[i]) (pieces 1..8 combined, 9..12 single) on host arrays.  The
  * reference has no counterpart (its quotients are fast_div, mertens_dr.hpp:80,
- * and its summands Piece1..SinglePiece4, :470-482). */
+ * and its summands Piece1..SinglePiece4, :470-482).  dr_debug_udiv_rcp runs the
+ * reciprocal-estimate quotient of the S1/S2 loops; it writes UINT64_MAX where
+ * d >= 2^32 or y/d >= 2^50 (outside that routine's domain). */
 int dr_debug_udiv(dr_ctx *ctx, const uint64_t *y, const uint64_t *d, int64_t n, uint64_t *q);
+int dr_debug_udiv_rcp(dr_ctx *ctx, const uint64_t *y, const uint64_t *d, int64_t n, uint64_t *q);
 int dr_debug_piece(dr_ctx *ctx, const int32_t *piece, const uint64_t *q, int64_t n, int64_t *out);
 
 /* Table build that allocates nothing.  It has no counterpart in the reference.

@@ -66,6 +66,41 @@ def test_udiv_s1_shapes(engine):
     assert all(g == y // d for y, d, g in zip(ys, ds, q))
 
 
+def _rcp_domain_pairs():
+    """(y, d) with d < 2^32 and y/d < 2^50: random, and y = q*d + {-1, 0, 1, d-1}
+    for q and d at the edges of the domain, where the double estimate of y/d is
+    least accurate relative to the integer boundaries."""
+    rng = random.Random(20261204)
+    pairs = []
+    for _ in range(150000):
+        d = max(1, rng.getrandbits(rng.choice([1, 6, 12, 20, 26, 30, 31, 32])))
+        q = rng.getrandbits(rng.choice([1, 10, 20, 33, 40, 45, 48, 49, 50]))
+        y = q * d + rng.randrange(d)
+        if y < 2**64 and (y >> 50) < d:
+            pairs.append((y, d))
+    for d in (1, 2, 3, 5, 6, 7, 2**20 - 1, 2**31 - 1, 2**31, 2**32 - 5, 2**32 - 1, 3037000493, 4000000000):
+        for q in (1, 2, 2**40 + 1, 2**49 - 1, 2**49, 2**50 - 2, 2**50 - 1, 10**15, 10**12 + 39):
+            for r in (-1, 0, 1, d - 1):
+                y = q * d + r
+                if 0 <= y < 2**64 and (y >> 50) < d:
+                    pairs.append((y, d))
+    return pairs
+
+
+def test_udiv_rcp_matches_floor(engine):
+    pairs = _rcp_domain_pairs()
+    ys, ds = zip(*pairs)
+    q = engine.debug_udiv(ys, ds, rcp=True)
+    bad = [(y, d, g) for (y, d), g in zip(pairs, q) if g != y // d]
+    assert not bad, bad[:5]
+
+
+def test_udiv_rcp_domain_flag(engine):
+    ys = [2**63, 2**62, 5, 2**50 * 7]
+    ds = [3, 2**32, 0, 7]
+    assert engine.debug_udiv(ys, ds, rcp=True) == [2**64 - 1] * 4
+
+
 def test_pieces_match_oracle(engine, oracle):
     rng = random.Random(5)
     qs = list(range(0, 300)) + [rng.getrandbits(b) for b in (20, 40, 53, 60, 62) for _ in range(200)]
