@@ -60,6 +60,24 @@ __device__ __forceinline__ u64 udiv_rcp(u64 y, double yd, uint32_t n, double r) 
     return qe + (u64)(i64)((int)(rem >= (i64)n) - (int)(rem < 0));
 }
 
+// 32-bit quotients of the S1 / S2 fast paths (n < 2^31 and floor(y/n) < 2^31).
+// qest: ceil(yd*r - 1/2) read from the low mantissa word of RU(yd*r + 2^52 - 1/2)
+// (one FMA; for y >= n the sum lies in [2^52, 2^53), where the spacing is 1).  yd*r
+// is within (y/n) * 2^-52 < 1/2 of y/n, so the estimate qp is floor(y/n) or
+// floor(y/n) + 1.  Callers divide only y >= n (every S1/S2 quotient is >= 1).
+// qfix: y - qp*n lies in [-n, n), so its low 32 bits, read as a signed integer,
+// say which one (n < 2^31); one IMAD and a sign bit replace the 64-bit remainder.
+constexpr double kQBias = 4503599627370495.5;  // 2^52 - 1/2
+
+__device__ __forceinline__ uint32_t qest(double yd, double r) {
+    return (uint32_t)__double2loint(__fma_ru(yd, r, kQBias));
+}
+
+__device__ __forceinline__ uint32_t qfix(uint32_t qp, uint32_t ylo, uint32_t n) {
+    const uint32_t d = ylo - qp * n;  // y - qp*n mod 2^32
+    return qp - (d >> 31);
+}
+
 __device__ __forceinline__ u64 udiv(u64 y, u64 d) {
     if (d >> 32) return y / d;  // divisor above 32 bits: rare, exact library path
     if ((y >> 32) == 0) return (uint32_t)y / (uint32_t)d;

@@ -1038,7 +1038,11 @@ int dr_debug_udiv_rcp(dr_ctx* c, const uint64_t* y, const uint64_t* d, int64_t n
     return debug_udiv(c, y, d, n, q, 1);
 }
 
-int dr_debug_piece(dr_ctx* c, const int32_t* piece, const uint64_t* q, int64_t n, int64_t* out) {
+int dr_debug_udiv32(dr_ctx* c, const uint64_t* y, const uint64_t* d, int64_t n, uint64_t* q) {
+    return debug_udiv(c, y, d, n, q, 2);
+}
+
+static int debug_piece(dr_ctx* c, const int32_t* piece, const uint64_t* q, int64_t n, int64_t* out, int fast) {
     if (!c || !piece || !q || !out || n < 0) return fail(DR_ERR_ARG, "bad argument");
     if (n == 0) return DR_OK;
     CU(cudaSetDevice(c->device));
@@ -1049,11 +1053,19 @@ int dr_debug_piece(dr_ctx* c, const int32_t* piece, const uint64_t* q, int64_t n
     int32_t* dp = (int32_t*)(dout + n);
     CU(cudaMemcpyAsync(dq, q, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream));
     CU(cudaMemcpyAsync(dp, piece, (size_t)n * 4, cudaMemcpyHostToDevice, c->stream));
-    launch_debug_piece(dp, dq, dout, n, c->stream);
+    launch_debug_piece(dp, dq, dout, n, fast, c->stream);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(out, dout, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
     CU(cudaStreamSynchronize(c->stream));
     return DR_OK;
+}
+
+int dr_debug_piece(dr_ctx* c, const int32_t* piece, const uint64_t* q, int64_t n, int64_t* out) {
+    return debug_piece(c, piece, q, n, out, 0);
+}
+
+int dr_debug_piece32(dr_ctx* c, const int32_t* piece, const uint64_t* q, int64_t n, int64_t* out) {
+    return debug_piece(c, piece, q, n, out, 1);
 }
 
 }  // extern "C"

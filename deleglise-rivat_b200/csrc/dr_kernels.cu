@@ -521,55 +521,84 @@ void launch_scan_u64(const u64* in, u64* out, u64 n, u64* tmp, size_t, cudaStrea
 // Persistent S1 / S2 kernel over the flattened op space.
 // ---------------------------------------------------------------------------
 
-// Code-shape knobs of the sums kernel (chosen by measurement on B200).
-#ifndef DRB_S1_INLINE
-#define DRB_S1_INLINE __device__ __forceinline__
-#endif
-#ifndef DRB_S2_INLINE
-#define DRB_S2_INLINE __device__ __forceinline__
-#endif
+// Code-shape knobs of the sums kernel (chosen by measurement on B200: 64
+// registers, 4 CTAs of 256 threads per SM).
 #ifndef DRB_SUMS_MINB
-#define DRB_SUMS_MINB 1
+#define DRB_SUMS_MINB 4
 #endif
 #ifndef DRB_S1_UNROLL
 #define DRB_S1_UNROLL 8
 #endif
 
 constexpr int kS1Unroll = DRB_S1_UNROLL;  // independent gathers in flight per lane
-constexpr int kS2Unroll = 2;
+
+// 1/n for the kS1Unroll divisors n = nfirst + nstep*k of a lane's group.  From
+// nfirst >= 2^14 on, only 1/nfirst is loaded; the others start from the first-order
+// Taylor value r0*(1 - k*nstep*r0), relative error (k*nstep/nfirst)^2 <= 2^-10.4,
+// and two Newton steps r += r*(1 - n*r) square that error twice (to below 2^-41,
+// on the FP64 pipe, which the loop leaves idle) -- far inside what the 32-bit
+// dense route needs (q <= u_dense < 2^31).  Below 2^14 every reciprocal is loaded.  This cuts the L2 traffic
+// of the reciprocal table by a factor kS1Unroll where the loop is bound by it.
+__device__ __forceinline__ void rcp_group(const double* rcp, u64 nfirst, u64 nstep, double* rv) {
+    if (nfirst >= (1u << 14)) {
+        const double r0 = __ldg(rcp + nfirst);
+        const double xr = (double)nstep * r0 * r0;
+        const double nd = (double)nfirst;
+        rv[0] = r0;
+#pragma unroll
+        for (int k = 1; k < kS1Unroll; ++k) {
+            const double nk = nd + (double)(nstep * k);  // exact
+            double r = __fma_rn(-(double)k, xr, r0);
+#pragma unroll
+            for (int it = 0; it < 2; ++it) r = __fma_rn(r, __fma_rn(-nk, r, 1.0), r);
+            rv[k] = r;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kS1Unroll; ++k) rv[k] = __ldg(rcp + nfirst + nstep * k);
+    }
+}
 
 // sum of M(floor(y/n)) over n = n0 + stride*i, i in [i0, i1), lanes interleaved.
 // Groups of kS1Unroll iterations issue their reciprocal loads, quotients and
-// table gathers back to back; a group whose divisors are all tabulated and
-// whose quotients all fall in the dense tier takes the branch-free path.
-DRB_S1_INLINE i64 s1_part(const SumsArgs& a, u64 y, i64 n0, int stride, u64 i0, u64 i1, int lane) {
-    // every q = floor(y/n) here is at most u_total < 2^42, so the reciprocal
-    // estimate (udiv_rcp) applies to every tabulated n
+// table gathers back to back.  A group whose divisors are tabulated and below
+// 2^31 and whose first (largest) quotient is in the dense tier -- q falls as n
+// grows, so then every quotient is -- runs on 32-bit quotients (qest/qfix); the
+// rest use the 64-bit routine (every q here is at most u_total < 2^42, inside
+// udiv_rcp's domain) or udiv above the tables.
+__device__ __forceinline__ i64 s1_part(const SumsArgs& a, u64 y, i64 n0, int stride, u64 i0, u64 i1, int lane) {
     i64 acc = 0;
     const u64 lim = (u64)a.inv_limit;
-    const u64 ud = (u64)a.T.u_dense;
+    const u64 lim31 = min(lim, (u64)0x7FFFFFFF);
     const u64 nstep = 32ull * (u64)stride;
     const double yd = __ull2double_rn(y);
+    const uint32_t ylo = (uint32_t)y;
+    const double dense_t = 4503599627370496.0 + (double)a.T.u_dense;  // 2^52 + u_dense
+    const int16_t* dMm1 = a.T.dM - 1;                                  // dMm1[q] = M(q)
     u64 i = i0 + lane;
     for (; i + 32 * (kS1Unroll - 1) < i1; i += 32 * kS1Unroll) {
         const u64 nfirst = (u64)n0 + (u64)stride * i;
         const u64 nlast = nfirst + nstep * (kS1Unroll - 1);
-        if (nlast <= lim) {
+        if (nlast <= lim31) {
             double rv[kS1Unroll];
-            u64 q[kS1Unroll];
+            rcp_group(a.rcp, nfirst, nstep, rv);
+            // t0 = 2^52 + qest of the first divisor: qest <= u_dense bounds q
+            const double t0 = __fma_ru(yd, rv[0], kQBias);
+            if (t0 <= dense_t) {
+                const uint32_t nf = (uint32_t)nfirst;
+                int32_t part = 0;
 #pragma unroll
-            for (int k = 0; k < kS1Unroll; ++k) rv[k] = __ldg(a.rcp + nfirst + nstep * k);
+                for (int k = 0; k < kS1Unroll; ++k) {
+                    const uint32_t qp = k == 0 ? (uint32_t)__double2loint(t0) : qest(yd, rv[k]);
+                    part += __ldg(dMm1 + qfix(qp, ylo, nf + (uint32_t)nstep * k));
+                }
+                acc += part;
+            } else {  // compressed tier (rare): exact tabulated reciprocals for udiv_rcp
 #pragma unroll
-            for (int k = 0; k < kS1Unroll; ++k) q[k] = udiv_rcp(y, yd, (uint32_t)(nfirst + nstep * k), rv[k]);
-            if (q[0] <= ud && q[kS1Unroll - 1] >= 1) {  // q falls with n: all in the dense tier
-                int32_t m[kS1Unroll];
-#pragma unroll
-                for (int k = 0; k < kS1Unroll; ++k) m[k] = __ldg(a.T.dM + (q[k] - 1));
-#pragma unroll
-                for (int k = 0; k < kS1Unroll; ++k) acc += m[k];
-            } else {
-#pragma unroll
-                for (int k = 0; k < kS1Unroll; ++k) acc += table_M(a.T, q[k]);
+                for (int k = 0; k < kS1Unroll; ++k) {
+                    const u64 n = nfirst + nstep * k;
+                    acc += table_M(a.T, udiv_rcp(y, yd, (uint32_t)n, __ldg(a.rcp + n)));
+                }
             }
         } else {
 #pragma unroll
@@ -635,8 +664,9 @@ __device__ __forceinline__ u64 s2_position(u64 y, double yd, const PieceCoef& pc
 }
 
 // sum of mu(j) * piece(floor(y/j)) for j in {6m+1, 6m+5} within [jlo, jhi],
-// m = jlo/6 + i, i in [i0, i1) of the piece's mcnt positions.  RCP: every j of
-// the range is below 2^32 and every y/j below 2^50 (udiv_rcp applies).
+// m = jlo/6 + i, i in [i0, i1) of the piece's mcnt positions (64-bit quotients).
+// RCP: every j of the range is below 2^32 and every y/j below 2^50 (udiv_rcp
+// applies).
 template <int KIND, bool RCP>
 __device__ __forceinline__ u64 s2_part(const SumsArgs& a, u64 y, const PieceCoef pc, i64 jlo, i64 jhi, u64 mcnt,
                                        u64 i0, u64 i1, int lane) {
@@ -644,35 +674,74 @@ __device__ __forceinline__ u64 s2_part(const SumsArgs& a, u64 y, const PieceCoef
     const double yd = __ull2double_rn(y);
     const u64 m0 = (u64)(jlo / 6);
     const u64 last = mcnt - 1;
-    u64 i = i0 + lane;
-    for (; i + 32 * (kS2Unroll - 1) < i1; i += 32 * kS2Unroll) {
-        uint4 w[kS2Unroll];
-        double2 iv[kS2Unroll];
-#pragma unroll
-        for (int k = 0; k < kS2Unroll; ++k) {
-            const u64 m = m0 + i + 32 * k;
-            w[k] = __ldg(a.T.wheel + (m >> 5));
-            iv[k] = __ldg(a.invw + m);
-        }
-#pragma unroll
-        for (int k = 0; k < kS2Unroll; ++k) {
-            const u64 ii = i + 32 * k;
-            acc += s2_position<KIND, RCP>(y, yd, pc, jlo, jhi, m0 + ii, ii == 0 || ii == last, w[k], iv[k]);
-        }
-    }
-    for (; i < i1; i += 32) {
+    for (u64 i = i0 + lane; i < i1; i += 32) {
         const u64 m = m0 + i;
         acc += s2_position<KIND, RCP>(y, yd, pc, jlo, jhi, m, i == 0 || i == last, __ldg(a.T.wheel + (m >> 5)),
-                                 __ldg(a.invw + m));
+                                      __ldg(a.invw + m));
     }
     return acc;
 }
 
-DRB_S2_INLINE u64 s2_dispatch(const SumsArgs& a, u64 y, int piece, i64 jlo, i64 jhi, u64 mcnt, u64 i0,
-                                        u64 i1, int lane) {
+// The summand on q < 2^31 in 32-bit arithmetic; sT[r] = piece(r), r < 12.
+template <int KIND>
+__device__ __forceinline__ int32_t piece32(int32_t a12, const int32_t* sT, uint32_t q) {
+    if (KIND == 1) return (int32_t)q;
+    if (KIND == 2) return (int32_t)((q + 1) >> 1);
+    if (KIND == 3) return (int32_t)(q & 1);
+    if (KIND == 4) return (int32_t)((q >> 2) + (q & 1));
+    const uint32_t k = q / 12u;
+    return a12 * (int32_t)k + sT[q - 12u * k];
+}
+
+// The same sum when every j of the range is below 2^31 and every y/j below 2^31:
+// 32-bit quotients (qest/qfix) and summands, mu(j) as a multiplier in {-1, 0, 1}
+// (both j of a position are evaluated, whatever their mu).  Lanes stride the
+// positions by 32, so each lane reads the same bit of every wheel word.
+template <int KIND>
+__device__ __forceinline__ u64 s2_fast(const SumsArgs& a, u64 y, int32_t a12, const int32_t* sT, i64 jlo, i64 jhi,
+                                       u64 mcnt, u64 i0, u64 i1, int lane) {
+    const double yd = __ull2double_rn(y);
+    const uint32_t ylo = (uint32_t)y;
+    const u64 m0 = (u64)(jlo / 6);
+    const u64 last = mcnt - 1;
+    const uint32_t b = (uint32_t)((m0 + i0 + (u64)lane) & 31u);
+    i64 acc = 0;
+    for (u64 i = i0 + lane; i < i1; i += 32) {
+        const u64 m = m0 + i;
+        const uint4 w = __ldg(a.T.wheel + (m >> 5));
+        const double2 iv = __ldg(a.invw + m);
+        int mu1 = (int)((w.x >> b) & 1u) - 2 * (int)((w.y >> b) & 1u);
+        int mu5 = (int)((w.z >> b) & 1u) - 2 * (int)((w.w >> b) & 1u);
+        const uint32_t j1 = (uint32_t)(6 * m + 1);
+        if (i == 0 || i == last) {  // only a piece's first and last position can stick out
+            if ((i64)j1 < jlo || (i64)j1 > jhi) mu1 = 0;
+            if ((i64)j1 + 4 < jlo || (i64)j1 + 4 > jhi) mu5 = 0;
+        }
+        const uint32_t q1 = qfix(qest(yd, iv.x), ylo, j1);
+        const uint32_t q5 = qfix(qest(yd, iv.y), ylo, j1 + 4u);
+        acc += (i64)mu1 * piece32<KIND>(a12, sT, q1);
+        acc += (i64)mu5 * piece32<KIND>(a12, sT, q5);
+    }
+    return (u64)acc;
+}
+
+// sT: the residue table of every piece in shared memory (sT[12*piece + r]).
+__device__ __forceinline__ u64 s2_dispatch(const SumsArgs& a, const int32_t* sT, u64 y, int piece, i64 jlo,
+                                           i64 jhi, u64 mcnt, u64 i0, u64 i1, int lane) {
     const PieceCoef pc = c_piece[piece];
     const u64 m0 = (u64)(jlo / 6);
     const u64 jmin = 6 * (m0 + i0) + 1, jmax = 6 * (m0 + i1) + 5;  // bounds every j of [i0, i1)
+    if (jmax < 0x7FFFFFFFull && (y >> 31) < jmin) {
+        const int32_t* T = sT + 12 * piece;
+        const int32_t a12 = (int32_t)pc.a;
+        switch (piece_kind(piece)) {
+        case 1: return s2_fast<1>(a, y, a12, T, jlo, jhi, mcnt, i0, i1, lane);
+        case 2: return s2_fast<2>(a, y, a12, T, jlo, jhi, mcnt, i0, i1, lane);
+        case 3: return s2_fast<3>(a, y, a12, T, jlo, jhi, mcnt, i0, i1, lane);
+        case 4: return s2_fast<4>(a, y, a12, T, jlo, jhi, mcnt, i0, i1, lane);
+        default: return s2_fast<0>(a, y, a12, T, jlo, jhi, mcnt, i0, i1, lane);
+        }
+    }
     if (jmax >> 32 || (y >> 50) >= jmin) return s2_part<0, false>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
     switch (piece_kind(piece)) {
     case 1: return s2_part<1, true>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
@@ -696,6 +765,12 @@ __device__ __forceinline__ u64 upper_slot(const u64* prefix, u64 n_slots, u64 o)
 
 __global__ void __launch_bounds__(256, DRB_SUMS_MINB) sums_kernel(const SumsArgs a) {
     __shared__ EvalDesc sdesc[8];  // one decoded evaluation per warp
+    __shared__ int32_t sT[13 * 12];  // piece(r) for r < 12, every piece
+    for (int t = threadIdx.x; t < 13 * 12; t += blockDim.x) {
+        const PieceCoef pc = c_piece[t / 12];
+        sT[t] = (int32_t)((pc.packed >> (5 * (t % 12))) & 31u) - 16;
+    }
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     EvalDesc& d = sdesc[threadIdx.x >> 5];
     const u64 total = a.prefix[a.n_slots];
@@ -763,7 +838,7 @@ __global__ void __launch_bounds__(256, DRB_SUMS_MINB) sums_kernel(const SumsArgs
                     s1 += sg > 0 ? (u64)part : (u64)(-part);
                 } else {
                     const int p = g - 2;
-                    const u64 part = s2_dispatch(a, y, d.piece0 + p, d.jlo[p], d.jhi[p], (u64)d.mcnt[p], a0 - sb,
+                    const u64 part = s2_dispatch(a, sT, y, d.piece0 + p, d.jlo[p], d.jhi[p], (u64)d.mcnt[p], a0 - sb,
                                                  a1 - sb, lane);
                     s2 += coef > 0 ? part : (u64)(0 - part);
                 }
@@ -874,21 +949,48 @@ void launch_table_sums(const TableView& T, i64 nwords, u64* out6, int sm_count, 
 // Test support: the device quotient and S2 summand on caller-chosen inputs.
 // ---------------------------------------------------------------------------
 // rcp = 0: udiv; rcp = 1: udiv_rcp with a device-computed reciprocal, ~0 where
-// (y, d) is outside its domain (d >= 2^32 or y/d >= 2^50)
+// (y, d) is outside its domain (d >= 2^32 or y/d >= 2^50); rcp = 2: the 32-bit
+// route of the S1/S2 fast paths (qest + qfix), ~0 where d >= 2^31, y/d >= 2^31 or
+// y < d (the fast paths only divide y by d <= y)
 __global__ void debug_udiv_kernel(const u64* y, const u64* d, u64* q, i64 n, int rcp) {
     const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const u64 yy = y[i], dd = d[i];
-    if (!rcp) q[i] = dd ? udiv(yy, dd) : 0;
-    else if (dd == 0 || (dd >> 32) || (yy >> 50) >= dd) q[i] = ~0ull;
-    else q[i] = udiv_rcp(yy, __ull2double_rn(yy), (uint32_t)dd, __drcp_rn((double)dd));
+    if (rcp == 0) q[i] = dd ? udiv(yy, dd) : 0;
+    else if (rcp == 1) {
+        if (dd == 0 || (dd >> 32) || (yy >> 50) >= dd) q[i] = ~0ull;
+        else q[i] = udiv_rcp(yy, __ull2double_rn(yy), (uint32_t)dd, __drcp_rn((double)dd));
+    } else {
+        if (dd == 0 || (dd >> 31) || (yy >> 31) >= dd || yy < dd) q[i] = ~0ull;
+        else q[i] = qfix(qest(__ull2double_rn(yy), __drcp_rn((double)dd)), (uint32_t)yy, (uint32_t)dd);
+    }
 }
 
-__global__ void debug_piece_kernel(const int32_t* piece, const u64* q, i64* out, i64 n) {
+// wide = 0: piece_eval (64-bit); wide = 1: piece32 of the S2 fast path on q < 2^31
+// (INT64_MIN for larger q)
+__global__ void debug_piece_kernel(const int32_t* piece, const u64* q, i64* out, i64 n, int fast) {
     const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) {
-        const int p = piece[i];
-        out[i] = (p >= 1 && p <= 12) ? piece_eval(c_piece[p], q[i]) : 0;
+    if (i >= n) return;
+    const int p = piece[i];
+    if (p < 1 || p > 12) {
+        out[i] = 0;
+    } else if (!fast) {
+        out[i] = piece_eval(c_piece[p], q[i]);
+    } else if (q[i] >> 31) {
+        out[i] = INT64_MIN;
+    } else {
+        const PieceCoef pc = c_piece[p];
+        int32_t T[12];
+        for (int r = 0; r < 12; ++r) T[r] = (int32_t)((pc.packed >> (5 * r)) & 31u) - 16;
+        const uint32_t v = (uint32_t)q[i];
+        const int32_t a12 = (int32_t)pc.a;
+        switch (piece_kind(p)) {
+        case 1: out[i] = piece32<1>(a12, T, v); break;
+        case 2: out[i] = piece32<2>(a12, T, v); break;
+        case 3: out[i] = piece32<3>(a12, T, v); break;
+        case 4: out[i] = piece32<4>(a12, T, v); break;
+        default: out[i] = piece32<0>(a12, T, v); break;
+        }
     }
 }
 
@@ -896,8 +998,8 @@ void launch_debug_udiv(const u64* y, const u64* d, u64* q, i64 n, int rcp, cudaS
     if (n > 0) debug_udiv_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(y, d, q, n, rcp);
 }
 
-void launch_debug_piece(const int32_t* piece, const u64* q, i64* out, i64 n, cudaStream_t s) {
-    if (n > 0) debug_piece_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(piece, q, out, n);
+void launch_debug_piece(const int32_t* piece, const u64* q, i64* out, i64 n, int fast, cudaStream_t s) {
+    if (n > 0) debug_piece_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(piece, q, out, n, fast);
 }
 
 }  // namespace drb

@@ -83,6 +83,6 @@ int record_error(int code, const char* msg);
 void sieve_kernel_attrs(size_t smem, int block, int* per_sm);
 void sums_kernel_occupancy(int block, int* per_sm);
 void launch_debug_udiv(const u64* y, const u64* d, u64* q, i64 n, int rcp, cudaStream_t s);
-void launch_debug_piece(const int32_t* piece, const u64* q, i64* out, i64 n, cudaStream_t s);
+void launch_debug_piece(const int32_t* piece, const u64* q, i64* out, i64 n, int fast, cudaStream_t s);
 
 }  // namespace drb

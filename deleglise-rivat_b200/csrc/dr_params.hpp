@@ -128,17 +128,18 @@ inline void ref_compressed_params(int64_t X, dr_params* p) {
     p->mu_limit = std::min(u_total, mu_limit);
 }
 
-// B200 policy (DR_POLICY_GPU), fitted to measured device times over
-// X = 10^12 .. 10^18 (table build ~4 ms per 10^9 values; S1 ~2.2 ms per 10^9
-// lookups; S2 ~3.8 ms per 10^9 wheel positions): the table is far cheaper to
-// build on the GPU than on the CPU, so u is raised to (X / ln ln X)^(2/3)
-// (the reference's fx = 1.0 without its 8e9 cap), cx = 1.2.  u is capped at
-// 2.5e11 values (~80 GB of compressed tier) and never below the endpoints.
+// B200 policy (DR_POLICY_GPU), fitted to a sweep of measured device times over
+// X = 10^14 .. 10^18 (fx in 0.15 .. 1, cx in 1 .. 2.1; table build ~3 ms per 10^9
+// values, S1 ~1.3 ms per 10^9 lookups, S2 ~3 ms per 10^9 wheel positions): the
+// table is far cheaper to build on the GPU than on the CPU, so u is raised to
+// 0.6 (X / ln ln X)^(2/3) -- the reference's u formula without its 8e9 cap --
+// and cx = 1.3.  u is capped at 2.5e11 values (~80 GB of compressed tier) and
+// never below the endpoints.
 inline void gpu_params(int64_t X, dr_params* p) {
     params_clear(p);
-    const double cx = 1.2;
+    const double cx = 1.3;
     const double loglogX = std::log(std::max(2.0, std::log((double)X)));
-    int64_t u = (int64_t)std::pow((double)X / loglogX, 2.0 / 3.0);
+    int64_t u = (int64_t)(0.6 * std::pow((double)X / loglogX, 2.0 / 3.0));
     const int64_t S = isqrt_i64(X);
     u = std::max(u, 3 * S);
     u = std::min<int64_t>(u, 250000000000LL);

@@ -136,8 +136,11 @@ def lib():
             "dr_table_checksums": (i32, [vp, ctypes.POINTER(TableSums)]),
             "dr_debug_udiv": (i32, [vp, ctypes.POINTER(u64), ctypes.POINTER(u64), i64, ctypes.POINTER(u64)]),
             "dr_debug_udiv_rcp": (i32, [vp, ctypes.POINTER(u64), ctypes.POINTER(u64), i64, ctypes.POINTER(u64)]),
+            "dr_debug_udiv32": (i32, [vp, ctypes.POINTER(u64), ctypes.POINTER(u64), i64, ctypes.POINTER(u64)]),
             "dr_debug_piece": (i32, [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(u64), i64,
                                      ctypes.POINTER(i64)]),
+            "dr_debug_piece32": (i32, [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(u64), i64,
+                                       ctypes.POINTER(i64)]),
             "dr_table_build_noalloc": (i32, [i32, vp, i64, i64, i64, vp, vp, vp, vp]),
             "dr_autotune_batch": (i32, [vp, ctypes.POINTER(i64), i64, i32, P, ctypes.POINTER(ctypes.c_double)]),
             "dr_mlp_create": (i32, [vp, u64, ctypes.POINTER(vp)]),
@@ -169,7 +172,8 @@ def exported_symbols() -> list:
         "dr_ctx_create", "dr_ctx_destroy", "dr_last_error", "dr_ctx_set_hbm_budget", "dr_device_info",
         "dr_default_params", "dr_check_params", "dr_table_bytes", "dr_query_bytes", "dr_mertens", "dr_mertens_batch",
         "dr_batch_checksums", "dr_table_build", "dr_table_read", "dr_table_read_wheel", "dr_table_checksums",
-        "dr_debug_udiv", "dr_debug_udiv_rcp", "dr_debug_piece", "dr_table_build_noalloc", "dr_autotune_batch",
+        "dr_debug_udiv", "dr_debug_udiv_rcp", "dr_debug_udiv32", "dr_debug_piece", "dr_debug_piece32",
+        "dr_table_build_noalloc", "dr_autotune_batch",
         "dr_mlp_create", "dr_mlp_destroy", "dr_mlp_num_params", "dr_mlp_set_weights", "dr_mlp_get_weights",
         "dr_mlp_forward", "dr_mlp_grad", "dr_mlp_train", "dr_tuner_features", "dr_tuner_params", "dr_tuner_propose",
     ]
@@ -306,23 +310,27 @@ class Engine:
         return mu
 
     # --- device arithmetic (test support) --------------------------------------
-    def debug_udiv(self, ys, ds, rcp: bool = False):
-        """floor(y/d) computed by the device quotient routine (rcp: the
-        reciprocal-estimate routine of the S1/S2 loops; 2^64-1 outside its domain)."""
+    def debug_udiv(self, ys, ds, rcp=False):
+        """floor(y/d) computed by a device quotient routine: the general one
+        (rcp False), the 64-bit reciprocal-estimate one (rcp True or "64"), or
+        the 32-bit one of the fast S1/S2 paths (rcp "32"); 2^64-1 outside the
+        routine's domain."""
         n = len(ys)
         Y = (ctypes.c_uint64 * n)(*[int(v) for v in ys])
         D = (ctypes.c_uint64 * n)(*[int(v) for v in ds])
         Q = (ctypes.c_uint64 * n)()
-        fn = lib().dr_debug_udiv_rcp if rcp else lib().dr_debug_udiv
+        fn = lib().dr_debug_udiv32 if rcp == "32" else lib().dr_debug_udiv_rcp if rcp else lib().dr_debug_udiv
         _check(fn(self._ctx, Y, D, n, Q))
         return list(Q)
 
-    def debug_piece(self, pieces, qs):
+    def debug_piece(self, pieces, qs, fast: bool = False):
+        """S2 summand piece(q): the 64-bit routine, or (fast) the 32-bit one of the
+        fast S2 path (INT64_MIN for q >= 2^31)."""
         n = len(qs)
         P = (ctypes.c_int32 * n)(*[int(v) for v in pieces])
         Q = (ctypes.c_uint64 * n)(*[int(v) for v in qs])
         O = (ctypes.c_int64 * n)()
-        _check(lib().dr_debug_piece(self._ctx, P, Q, n, O))
+        _check((lib().dr_debug_piece32 if fast else lib().dr_debug_piece)(self._ctx, P, Q, n, O))
         return list(O)
 
     def table_checksums(self) -> tuple:

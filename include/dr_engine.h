@@ -172,6 +172,11 @@ int dr_table_read_wheel(dr_ctx *ctx, int64_t first, int64_t count, int8_t *mu);
 int dr_debug_udiv(dr_ctx *ctx, const uint64_t *y, const uint64_t *d, int64_t n, uint64_t *q);
 int dr_debug_udiv_rcp(dr_ctx *ctx, const uint64_t *y, const uint64_t *d, int64_t n, uint64_t *q);
 int dr_debug_piece(dr_ctx *ctx, const int32_t *piece, const uint64_t *q, int64_t n, int64_t *out);
+/* The 32-bit routes of the S1/S2 fast paths: dr_debug_udiv32 writes UINT64_MAX
+ * where d >= 2^31, y/d >= 2^31 or y < d, dr_debug_piece32 writes INT64_MIN where
+ * q >= 2^31 (outside their domains).  No counterpart in the reference. */
+int dr_debug_udiv32(dr_ctx *ctx, const uint64_t *y, const uint64_t *d, int64_t n, uint64_t *q);
+int dr_debug_piece32(dr_ctx *ctx, const int32_t *piece, const uint64_t *q, int64_t n, int64_t *out);
 
 /* Table build that allocates nothing.  It has no counterpart in the reference.
  *

@@ -113,3 +113,53 @@ def test_pieces_match_oracle(engine, oracle):
     got = engine.debug_piece(pieces, vals)
     for p, q, g in zip(pieces, vals, got):
         assert g == oracle.piece(p, q), (p, q, g)
+
+
+def _fast_domain_pairs():
+    """(y, d) with d <= y, d < 2^31 and y/d < 2^31 (the 32-bit route of the fast
+    S1/S2 paths): random, and y = q*d + {-1, 0, 1, d-1} at the domain's edges, where
+    the remainder's low 32 bits and the estimate's rounding are tightest."""
+    rng = random.Random(20261205)
+    pairs = []
+    for _ in range(150000):
+        d = max(1, rng.getrandbits(rng.choice([1, 6, 12, 20, 26, 30, 31])))
+        q = rng.getrandbits(rng.choice([1, 10, 20, 26, 29, 30, 31]))
+        y = q * d + rng.randrange(d)
+        if d <= y and (y >> 31) < d:
+            pairs.append((y, d))
+    for d in (1, 2, 3, 5, 6, 7, 12, 2**16 + 1, 2**20 - 1, 2**30 + 3, 2**31 - 2, 2**31 - 1):
+        for q in (1, 2, 11, 12, 13, 2**20 + 1, 2**30, 2**31 - 2, 2**31 - 1):
+            for r in (-1, 0, 1, d - 1):
+                y = q * d + r
+                if d <= y and (y >> 31) < d:
+                    pairs.append((y, d))
+    return pairs
+
+
+def test_udiv32_matches_floor(engine):
+    pairs = _fast_domain_pairs()
+    ys, ds = zip(*pairs)
+    q = engine.debug_udiv(ys, ds, rcp="32")
+    bad = [(y, d, g) for (y, d), g in zip(pairs, q) if g != y // d]
+    assert not bad, bad[:5]
+
+
+def test_udiv32_domain_flag(engine):
+    ys = [2**31 * 5, 7, 2**40, 3, 0, 4]
+    ds = [5, 2**31, 3, 0, 1, 5]
+    assert engine.debug_udiv(ys, ds, rcp="32") == [2**64 - 1] * 6
+
+
+def test_pieces32_match_oracle(engine, oracle):
+    rng = random.Random(6)
+    qs = list(range(0, 300)) + [rng.getrandbits(b) for b in (12, 20, 28, 30, 31) for _ in range(300)]
+    qs += [2**31 - 12, 2**31 - 2, 2**31 - 1]
+    pieces, vals = [], []
+    for p in range(1, 13):
+        for q in qs:
+            pieces.append(p)
+            vals.append(q)
+    got = engine.debug_piece(pieces, vals, fast=True)
+    for p, q, g in zip(pieces, vals, got):
+        assert g == oracle.piece(p, q), (p, q, g)
+    assert engine.debug_piece([1, 8], [2**31, 2**40], fast=True) == [-(2**63)] * 2

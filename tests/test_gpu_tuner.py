@@ -6,7 +6,7 @@
 * proposals pass the endpoint-coverage check or fall back to the reference
   heuristic; every proposal gives the exact M(X);
 * with the committed trained weights the proposal beats the reference's
-  default heuristic at X = 10^16 (the gain of the learned part).
+  default heuristic at X = 3*10^16 (the gain of the learned part).
 """
 import json
 import os
@@ -72,20 +72,23 @@ def test_proposal_and_fallback(engine):
 
 @pytest.mark.skipif(not os.path.exists(WEIGHTS), reason="trained weights not committed")
 def test_trained_tuner_beats_default_heuristic(engine):
+    """At X = 3*10^16 (M pinned by the reference engine's own run,
+    tests/golden/m30000000000000000.json) the proposal of the committed weights
+    is at least 5% faster on the device than the reference's default heuristic."""
     with open(WEIGHTS) as f:
         w = np.array(json.load(f)["weights"], dtype=np.float32)
     mlp = dr_b200.MLP(engine)
     mlp.set_weights(w)
-    X = 10**16
+    X = 3 * 10**16
     p, fb = mlp.propose(X, 160 * 2**30)
     assert not fb
     d = dr_b200.default_params(X, dr_b200.POLICY_REFERENCE)
 
     def t(params):
         best = None
-        for _ in range(3):
+        for _ in range(2):
             r = engine.mertens(X, params)
-            assert r.M == -3195437
+            assert r.M == -1493402
             v = r.stats.table_ms + r.stats.plan_ms + r.stats.sums_ms
             best = v if best is None else min(best, v)
         return best
