@@ -464,7 +464,8 @@ int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq,
     launch_direct((const QueryDev*)c->queries.p, qn, T, (u64*)c->acc.p, c->stream);
     int launches = 1;
     if (slots > 0) {
-        launch_inverse((double*)c->inv.p, inv_limit, (double2*)c->invw.p, invw_count, c->sm_count, c->stream);
+        launch_inverse((double*)c->inv.p, inv_limit, (double2*)c->invw.p, invw_count, T.wheel, c->sm_count,
+                       c->stream);
         launch_plan((const QueryDev*)c->queries.p, qn, T, slots, (u64*)c->ops.p, (u64*)c->acc.p, (i64*)c->counts.p,
                     c->sm_count, c->stream);
         launch_scan_u64((const u64*)c->ops.p, (u64*)c->prefix.p, slots, (u64*)c->scan_tmp.p,

@@ -665,8 +665,8 @@ __device__ __forceinline__ u64 s2_position(u64 y, double yd, const PieceCoef& pc
 
 // sum of mu(j) * piece(floor(y/j)) for j in {6m+1, 6m+5} within [jlo, jhi],
 // m = jlo/6 + i, i in [i0, i1) of the piece's mcnt positions (64-bit quotients).
-// RCP: every j of the range is below 2^32 and every y/j below 2^50 (udiv_rcp
-// applies).
+// RCP: every j of the range is below 2^32 and every y/j below 2^48 (udiv_rcp
+// applies to invw's reciprocals).
 template <int KIND, bool RCP>
 __device__ __forceinline__ u64 s2_part(const SumsArgs& a, u64 y, const PieceCoef pc, i64 jlo, i64 jhi, u64 mcnt,
                                        u64 i0, u64 i1, int lane) {
@@ -693,10 +693,32 @@ __device__ __forceinline__ int32_t piece32(int32_t a12, const int32_t* sT, uint3
     return a12 * (int32_t)k + sT[q - 12u * k];
 }
 
+// mu(j) from the low mantissa bits of invw's reciprocal (inverse_kernel)
+__device__ __forceinline__ int32_t mu_code(double r) {
+    return (int32_t)((uint32_t)__double2loint(r) << 30) >> 30;
+}
+
+__device__ __forceinline__ i64 mad_wide(int32_t a, int32_t b, i64 c) {
+    i64 r;
+    asm("mad.wide.s32 %0, %1, %2, %3;" : "=l"(r) : "r"(a), "r"(b), "l"(c));
+    return r;
+}
+
+// mu(j) * piece(floor(y/j)) for the two j of a position, j1 = 6m+1 and j1 + 4,
+// on the 32-bit route; take1/take5 clear j outside the piece (edge positions)
+template <int KIND>
+__device__ __forceinline__ i64 s2_pair32(i64 acc, double yd, uint32_t ylo, int32_t a12, const int32_t* sT,
+                                         uint32_t j1, double2 iv, bool take1 = true, bool take5 = true) {
+    const int32_t mu1 = take1 ? mu_code(iv.x) : 0, mu5 = take5 ? mu_code(iv.y) : 0;
+    acc = mad_wide(mu1, piece32<KIND>(a12, sT, qfix(qest(yd, iv.x), ylo, j1)), acc);
+    return mad_wide(mu5, piece32<KIND>(a12, sT, qfix(qest(yd, iv.y), ylo, j1 + 4u)), acc);
+}
+
 // The same sum when every j of the range is below 2^31 and every y/j below 2^31:
-// 32-bit quotients (qest/qfix) and summands, mu(j) as a multiplier in {-1, 0, 1}
-// (both j of a position are evaluated, whatever their mu).  Lanes stride the
-// positions by 32, so each lane reads the same bit of every wheel word.
+// 32-bit quotients (qest/qfix) and summands, mu(j) from invw as a multiplier in
+// {-1, 0, 1} (both j of a position are evaluated, whatever their mu).  The
+// piece's first and last positions -- the only ones that can hold a j outside
+// [jlo, jhi] -- are peeled off to lanes 0 and 1.
 template <int KIND>
 __device__ __forceinline__ u64 s2_fast(const SumsArgs& a, u64 y, int32_t a12, const int32_t* sT, i64 jlo, i64 jhi,
                                        u64 mcnt, u64 i0, u64 i1, int lane) {
@@ -704,23 +726,24 @@ __device__ __forceinline__ u64 s2_fast(const SumsArgs& a, u64 y, int32_t a12, co
     const uint32_t ylo = (uint32_t)y;
     const u64 m0 = (u64)(jlo / 6);
     const u64 last = mcnt - 1;
-    const uint32_t b = (uint32_t)((m0 + i0 + (u64)lane) & 31u);
     i64 acc = 0;
-    for (u64 i = i0 + lane; i < i1; i += 32) {
-        const u64 m = m0 + i;
-        const uint4 w = __ldg(a.T.wheel + (m >> 5));
-        const double2 iv = __ldg(a.invw + m);
-        int mu1 = (int)((w.x >> b) & 1u) - 2 * (int)((w.y >> b) & 1u);
-        int mu5 = (int)((w.z >> b) & 1u) - 2 * (int)((w.w >> b) & 1u);
-        const uint32_t j1 = (uint32_t)(6 * m + 1);
-        if (i == 0 || i == last) {  // only a piece's first and last position can stick out
-            if ((i64)j1 < jlo || (i64)j1 > jhi) mu1 = 0;
-            if ((i64)j1 + 4 < jlo || (i64)j1 + 4 > jhi) mu5 = 0;
+    const u64 b0 = max(i0, (u64)1), b1 = min(i1, last);  // interior positions [b0, b1)
+    const u64 i = b0 + (u64)lane;
+    if (i < b1) {
+        const uint32_t cnt = (uint32_t)((b1 - i + 31) >> 5);
+        const double2* p = a.invw + (m0 + i);
+        const uint32_t j1 = (uint32_t)(6 * (m0 + i) + 1);
+        for (uint32_t t = 0; t < cnt; ++t)
+            acc = s2_pair32<KIND>(acc, yd, ylo, a12, sT, j1 + 192u * t, __ldg(p + 32u * t));
+    }
+    if (lane < 2) {
+        const u64 e = lane == 0 ? 0 : last;
+        if (e >= i0 && e < i1 && (lane == 0 || last != 0)) {
+            const u64 m = m0 + e;
+            const i64 j1 = (i64)(6 * m + 1), j5 = j1 + 4;
+            acc = s2_pair32<KIND>(acc, yd, ylo, a12, sT, (uint32_t)j1, __ldg(a.invw + m), j1 >= jlo && j1 <= jhi,
+                                  j5 >= jlo && j5 <= jhi);
         }
-        const uint32_t q1 = qfix(qest(yd, iv.x), ylo, j1);
-        const uint32_t q5 = qfix(qest(yd, iv.y), ylo, j1 + 4u);
-        acc += (i64)mu1 * piece32<KIND>(a12, sT, q1);
-        acc += (i64)mu5 * piece32<KIND>(a12, sT, q5);
     }
     return (u64)acc;
 }
@@ -742,7 +765,9 @@ __device__ __forceinline__ u64 s2_dispatch(const SumsArgs& a, const int32_t* sT,
         default: return s2_fast<0>(a, y, a12, T, jlo, jhi, mcnt, i0, i1, lane);
         }
     }
-    if (jmax >> 32 || (y >> 50) >= jmin) return s2_part<0, false>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
+    // invw's reciprocals carry mu in their two low bits (up to 3.5 ulp from 1/j):
+    // udiv_rcp's +-1 correction then covers y/j < 2^48, not its full 2^50
+    if (jmax >> 32 || (y >> 48) >= jmin) return s2_part<0, false>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
     switch (piece_kind(piece)) {
     case 1: return s2_part<1, true>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
     case 2: return s2_part<2, true>(a, y, pc, jlo, jhi, mcnt, i0, i1, lane);
@@ -856,19 +881,33 @@ __global__ void __launch_bounds__(256, DRB_SUMS_MINB) sums_kernel(const SumsArgs
     }
 }
 
-// rcp[n] = RN(1/n) for 1 <= n <= inv_limit; invw[m] = {rcp(6m+1), rcp(6m+5)}.
-__global__ void inverse_kernel(double* rcp, i64 inv_limit, double2* invw, i64 invw_count) {
+// rcp[n] = RN(1/n) for 1 <= n <= inv_limit.  invw[m] = {rcp(6m+1), rcp(6m+5)} with
+// mu(j) in the two low mantissa bits (mu & 3: 0, 1, or 3 for -1), so the S2 loops
+// read j's reciprocal and its Mobius value with one load; the three ulp this may
+// move 1/j are far inside what the S2 quotient routes tolerate (mu_code, s2_part).
+__device__ __forceinline__ double rcp_with_mu(u64 j, const uint4* wheel) {
+    const u64 m = j / 6u;
+    const uint4 w = __ldg(wheel + (m >> 5));
+    const uint32_t b = (uint32_t)(m & 31u);
+    const bool five = (j - 6u * m) == 5u;
+    const uint32_t nz = ((five ? w.z : w.x) >> b) & 1u, ng = ((five ? w.w : w.y) >> b) & 1u;
+    const u64 bits = (u64)__double_as_longlong(__drcp_rn((double)j));
+    return __longlong_as_double((long long)((bits & ~3ull) | (u64)(nz | (ng << 1))));
+}
+
+__global__ void inverse_kernel(double* rcp, i64 inv_limit, double2* invw, i64 invw_count, const uint4* wheel) {
     const i64 stride = (i64)gridDim.x * blockDim.x;
     const i64 t0 = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     for (i64 n = t0; n <= inv_limit; n += stride) rcp[n] = n ? __drcp_rn((double)n) : 0.0;
     for (i64 m = t0; m < invw_count; m += stride)
-        invw[m] = make_double2(__drcp_rn((double)(6 * m + 1)), __drcp_rn((double)(6 * m + 5)));
+        invw[m] = make_double2(rcp_with_mu((u64)(6 * m + 1), wheel), rcp_with_mu((u64)(6 * m + 5), wheel));
 }
 
-void launch_inverse(double* rcp, i64 inv_limit, double2* invw, i64 invw_count, int sm_count, cudaStream_t s) {
+void launch_inverse(double* rcp, i64 inv_limit, double2* invw, i64 invw_count, const uint4* wheel, int sm_count,
+                    cudaStream_t s) {
     const i64 work = std::max<i64>(inv_limit + 1, invw_count);
     const int grid = (int)std::min<i64>((work + 255) / 256, (i64)sm_count * 16);
-    inverse_kernel<<<std::max(grid, 1), 256, 0, s>>>(rcp, inv_limit, invw, invw_count);
+    inverse_kernel<<<std::max(grid, 1), 256, 0, s>>>(rcp, inv_limit, invw, invw_count, wheel);
 }
 
 void sums_kernel_occupancy(int block, int* per_sm) {

@@ -44,7 +44,7 @@ struct SumsArgs {
     int chunk_log2;     // 0: chosen on the device from the total
     const double* rcp;       // rcp[n] = RN(1/n), 1 <= n <= inv_limit (< 2^32)
     i64 inv_limit;
-    const double2* invw;     // invw[m] = {rcp(6m+1), rcp(6m+5)}, m < invw_count
+    const double2* invw;     // invw[m] = {rcp(6m+1), rcp(6m+5)} with mu(j) in the low bits, m < invw_count
     i64 invw_count;
 };
 
@@ -70,7 +70,8 @@ void launch_scan_u64(const u64* in, u64* out, u64 n, u64* tmp, size_t tmp_elems,
 size_t scan_u64_tmp_elems(u64 n);
 void launch_sums(const SumsArgs& a, int grid, int block, cudaStream_t s);
 // Reciprocal tables shared by every evaluation of a launch.
-void launch_inverse(double* rcp, i64 inv_limit, double2* invw, i64 invw_count, int sm_count, cudaStream_t s);
+void launch_inverse(double* rcp, i64 inv_limit, double2* invw, i64 invw_count, const uint4* wheel, int sm_count,
+                    cudaStream_t s);
 void launch_direct(const QueryDev* q, int nq, const TableView& T, u64* acc, cudaStream_t s);
 void launch_table_read(const TableView& T, i64 first, i64 count, int32_t* M, int8_t* mu, int8_t* wheel_mu,
                        cudaStream_t s);
