@@ -532,83 +532,98 @@ void launch_scan_u64(const u64* in, u64* out, u64 n, u64* tmp, size_t, cudaStrea
 
 constexpr int kS1Unroll = DRB_S1_UNROLL;  // independent gathers in flight per lane
 
-// 1/n for the kS1Unroll divisors n = nfirst + nstep*k of a lane's group.  From
-// nfirst >= 2^14 on, only 1/nfirst is loaded; the others start from the first-order
-// Taylor value r0*(1 - k*nstep*r0), relative error (k*nstep/nfirst)^2 <= 2^-10.4,
-// and two Newton steps r += r*(1 - n*r) square that error twice (to below 2^-41,
-// on the FP64 pipe, which the loop leaves idle) -- far inside what the 32-bit
-// dense route needs (q <= u_dense < 2^31).  Below 2^14 every reciprocal is loaded.  This cuts the L2 traffic
-// of the reciprocal table by a factor kS1Unroll where the loop is bound by it.
-__device__ __forceinline__ void rcp_group(const double* rcp, u64 nfirst, u64 nstep, double* rv) {
+// Exact double of a 32-bit integer on the FP64 pipe (the conversion
+// instructions run on the narrow XU pipe): the low mantissa word of 2^52 + v.
+__device__ __forceinline__ double u32_to_double(uint32_t v) {
+    return __hiloint2double(0x43300000, (int)v) - 4503599627370496.0;
+}
+
+// 1/n for the kS1Unroll divisors n = nfirst + nstep*k of a lane's group
+// (nfirst + nstep*(kS1Unroll-1) < 2^31).  From nfirst >= 2^14 on, only 1/nfirst
+// is loaded; the others start from the first-order Taylor value r0*(1 -
+// k*nstep*r0), relative error (k*nstep/nfirst)^2 <= 2^-10.4, and two Newton steps
+// r += r*(1 - n*r) square that error twice (to below 2^-41, on the FP64 pipe,
+// which the loop leaves idle) -- far inside what the 32-bit dense route needs
+// (q <= u_dense < 2^31).  Below 2^14 every reciprocal is loaded.  This cuts the
+// L2 traffic of the reciprocal table by a factor kS1Unroll where the loop is
+// bound by it.
+__device__ __forceinline__ void rcp_group(const double* rcp, uint32_t nfirst, uint32_t nstep, double nstep_d,
+                                          double* rv) {
     if (nfirst >= (1u << 14)) {
         const double r0 = __ldg(rcp + nfirst);
-        const double xr = (double)nstep * r0 * r0;
-        const double nd = (double)nfirst;
+        const double xr = nstep_d * r0 * r0;
+        const double nd = u32_to_double(nfirst);
         rv[0] = r0;
 #pragma unroll
         for (int k = 1; k < kS1Unroll; ++k) {
-            const double nk = nd + (double)(nstep * k);  // exact
+            const double nk = __fma_rn((double)k, nstep_d, nd);  // exact
             double r = __fma_rn(-(double)k, xr, r0);
 #pragma unroll
             for (int it = 0; it < 2; ++it) r = __fma_rn(r, __fma_rn(-nk, r, 1.0), r);
             rv[k] = r;
         }
     } else {
+        const double* p = rcp + nfirst;
 #pragma unroll
-        for (int k = 0; k < kS1Unroll; ++k) rv[k] = __ldg(rcp + nfirst + nstep * k);
+        for (int k = 0; k < kS1Unroll; ++k) rv[k] = __ldg(p + nstep * (uint32_t)k);
     }
 }
 
 // sum of M(floor(y/n)) over n = n0 + stride*i, i in [i0, i1), lanes interleaved.
-// Groups of kS1Unroll iterations issue their reciprocal loads, quotients and
-// table gathers back to back.  A group whose divisors are tabulated and below
-// 2^31 and whose first (largest) quotient is in the dense tier -- q falls as n
-// grows, so then every quotient is -- runs on 32-bit quotients (qest/qfix); the
-// rest use the 64-bit routine (every q here is at most u_total < 2^42, inside
-// udiv_rcp's domain) or udiv above the tables.
+// Each lane walks groups of kS1Unroll of its divisors (n, n + 32*stride, ...)
+// whose reciprocal loads, quotients and table gathers issue back to back.  A group
+// whose divisors are tabulated and below 2^31 and whose first (largest) quotient
+// is in the dense tier -- q falls as n grows, so then every quotient is -- runs on
+// 32-bit quotients (qest/qfix); the rest use the 64-bit routine (every q here is
+// at most u_total < 2^42, inside udiv_rcp's domain) or udiv above the tables.
 __device__ __forceinline__ i64 s1_part(const SumsArgs& a, u64 y, i64 n0, int stride, u64 i0, u64 i1, int lane) {
     i64 acc = 0;
     const u64 lim = (u64)a.inv_limit;
     const u64 lim31 = min(lim, (u64)0x7FFFFFFF);
-    const u64 nstep = 32ull * (u64)stride;
+    const uint32_t nstep = 32u * (uint32_t)stride;
+    const double nstep_d = u32_to_double(nstep);
     const double yd = __ull2double_rn(y);
     const uint32_t ylo = (uint32_t)y;
     const double dense_t = 4503599627370496.0 + (double)a.T.u_dense;  // 2^52 + u_dense
     const int16_t* dMm1 = a.T.dM - 1;                                  // dMm1[q] = M(q)
-    u64 i = i0 + lane;
-    for (; i + 32 * (kS1Unroll - 1) < i1; i += 32 * kS1Unroll) {
-        const u64 nfirst = (u64)n0 + (u64)stride * i;
-        const u64 nlast = nfirst + nstep * (kS1Unroll - 1);
+    const u64 il = i0 + (u64)lane;
+    // this lane's full groups: il + 32*kS1Unroll*g + 32*(kS1Unroll-1) < i1
+    const u64 span = 32ull * (kS1Unroll - 1);
+    const uint32_t groups = il + span < i1 ? (uint32_t)((i1 - il - span - 1) / (32ull * kS1Unroll) + 1) : 0u;
+    const u64 gstep = (u64)nstep * kS1Unroll;
+    u64 nfirst = (u64)n0 + (u64)stride * il;
+    for (uint32_t g = 0; g < groups; ++g, nfirst += gstep) {
+        const u64 nlast = nfirst + (u64)nstep * (kS1Unroll - 1);
         if (nlast <= lim31) {
+            const uint32_t nf = (uint32_t)nfirst;
             double rv[kS1Unroll];
-            rcp_group(a.rcp, nfirst, nstep, rv);
+            rcp_group(a.rcp, nf, nstep, nstep_d, rv);
             // t0 = 2^52 + qest of the first divisor: qest <= u_dense bounds q
             const double t0 = __fma_ru(yd, rv[0], kQBias);
             if (t0 <= dense_t) {
-                const uint32_t nf = (uint32_t)nfirst;
                 int32_t part = 0;
 #pragma unroll
                 for (int k = 0; k < kS1Unroll; ++k) {
                     const uint32_t qp = k == 0 ? (uint32_t)__double2loint(t0) : qest(yd, rv[k]);
-                    part += __ldg(dMm1 + qfix(qp, ylo, nf + (uint32_t)nstep * k));
+                    part += __ldg(dMm1 + qfix(qp, ylo, nf + nstep * (uint32_t)k));
                 }
                 acc += part;
             } else {  // compressed tier (rare): exact tabulated reciprocals for udiv_rcp
 #pragma unroll
                 for (int k = 0; k < kS1Unroll; ++k) {
-                    const u64 n = nfirst + nstep * k;
-                    acc += table_M(a.T, udiv_rcp(y, yd, (uint32_t)n, __ldg(a.rcp + n)));
+                    const uint32_t n = nf + nstep * (uint32_t)k;
+                    acc += table_M(a.T, udiv_rcp(y, yd, n, __ldg(a.rcp + n)));
                 }
             }
         } else {
 #pragma unroll
             for (int k = 0; k < kS1Unroll; ++k) {
-                const u64 n = nfirst + nstep * k;
+                const u64 n = nfirst + (u64)nstep * k;
                 acc += table_M(a.T, n <= lim ? udiv_rcp(y, yd, (uint32_t)n, __ldg(a.rcp + n)) : udiv(y, n));
             }
         }
     }
-    for (; i < i1; i += 32) {
+    for (u64 i = il + 32ull * kS1Unroll * groups; i < i1; i += 32) {
         const u64 n = (u64)n0 + (u64)stride * i;
         acc += table_M(a.T, n <= lim ? udiv_rcp(y, yd, (uint32_t)n, __ldg(a.rcp + n)) : udiv(y, n));
     }
