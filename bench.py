@@ -355,9 +355,9 @@ def run_engine(args, world, rank, local):
     alg = 2 * s0_.s1_ops + 0.5 * s0_.s2_ops
     achieved = alg / (sums / 1e3) / 1e9
     # DRAM traffic: ncu dram__bytes_read.sum + dram__bytes_write.sum of sums_kernel
-    # measured at M(10^15) (profiles/sums_kernel_m1e15.md): 21.09 GB for 1.063e10
-    # ops = 1.98 B per op, scaled by this launch's op count (an estimate).
-    traffic = 1.98 * (s0_.s1_ops + s0_.s2_ops)
+    # measured at M(10^15) (profiles/sums_kernel_m1e15.md): 19.62 GB for 1.319e10
+    # ops = 1.49 B per op, scaled by this launch's op count (an estimate).
+    traffic = 1.49 * (s0_.s1_ops + s0_.s2_ops)
     line = {
         "metric": "sec per M(10^16)" if X == X_HEADLINE else f"sec per M({X})", "value": value, "unit": "s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_per * 1e3,
@@ -378,7 +378,7 @@ def run_engine(args, world, rank, local):
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                      "traffic_basis": "ncu DRAM bytes per op at M(10^15), scaled by op count",
                      "ops": {"s1_lookups": s0_.s1_ops, "s2_positions": s0_.s2_ops},
-                     "note": "integer-issue bound (exact quotients + gathers); S1 lookups + S2 positions per second",
+                     "note": "bound by L2 sector throughput of the S1 table gathers (lts 61-77%), not HBM; ops_per_s = S1 lookups + S2 positions per second",
                      "ops_per_s": (s0_.s1_ops + s0_.s2_ops) / (sums / 1e3)},
         "clocks": clocks.summary(),
         "batched": batch,
