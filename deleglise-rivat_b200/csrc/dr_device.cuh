@@ -191,7 +191,28 @@ struct QueryDev {
     i64 N;          // X / u
     i64 nc;         // candidates k <= N coprime to 6
     u64 slot_base;  // first global evaluation slot of this query
+    u64 win;        // S1 window length W (a power of two; 0: no windowed S1)
+    u64 win_max;    // windows w < win_max lie in the dense tier ((w+1)*W <= u_dense < 2^31)
+    u64 inv_limit;  // largest tabulated S1 reciprocal 1/n
 };
+
+#ifndef DRB_WIN_MIN
+#define DRB_WIN_MIN 64  // lookups of a segment in its last window (a power of two)
+#endif
+
+// Windowed S1 (s1win_kernel): the S1 lookups M(q) of an S1 segment with q below a
+// cut are summed window by window (q in [w*W, (w+1)*W), the window of the M table in
+// shared memory), the ones above it by the sums kernel.  The cut, a multiple of W,
+// sits where one window still holds about 64 of the segment's lookups
+// (y*W / (stride*Q^2) = 64), capped by the dense tier; it is returned as the
+// number of windowed windows.  IEEE operations only, so every kernel computes the
+// same cut.
+__device__ __forceinline__ u64 s1_win_count(u64 y, int stride, u64 W, u64 win_max) {
+    if (W == 0) return 0;
+    const double v = __dmul_rn(__ull2double_rn(y), (double)W / ((double)DRB_WIN_MIN * (double)stride));  // exact
+    const u64 wc = __double2ull_rz(__dmul_rn(__dsqrt_rn(v), 1.0 / (double)W));
+    return wc < win_max ? wc : win_max;
+}
 
 // Split point A = floor(cx * sqrt(y)) clamped to [1, y-1] (mertens_dr.hpp:1491-1493,
 // 1528-1533).  It is a parameter, not part of any sum: every A in range gives the
@@ -220,7 +241,9 @@ struct EvalDesc {
     int nseg;       // 2 + npieces
     i64 A, B, ky, ky2;
     i64 s1_n0[2];
-    i64 s1_cnt[2];
+    i64 s1_cnt[2];   // lookups of each S1 segment left to the sums kernel
+    i64 s1_full[2];  // all lookups of each S1 segment
+    u64 s1_wc[2];    // windows of each S1 segment summed by s1win_kernel
     int s1_stride[2];
     int s1_sign[2];
     i64 jlo[8], jhi[8];
@@ -308,6 +331,21 @@ __device__ inline void decode_eval(const QueryDev& Q, const TableView& T, i64 c,
         d.jlo[7] = B + 1;  d.jhi[7] = A;
     }
     d.nseg = 2 + d.npieces;
+    // windowed S1: the lookups with q < wc*W, i.e. n > y/(wc*W), go to s1win_kernel
+    for (int g = 0; g < 2; ++g) {
+        d.s1_full[g] = d.s1_cnt[g];
+        d.s1_wc[g] = 0;
+        const i64 cnt = d.s1_cnt[g];
+        if (cnt <= 0 || Q.win == 0) continue;
+        const i64 nlast = d.s1_n0[g] + (i64)d.s1_stride[g] * (cnt - 1);
+        // the windowed kernel divides on the 32-bit route with tabulated reciprocals
+        if (nlast >= (1ll << 31) || (u64)nlast > Q.inv_limit) continue;
+        const u64 wc = s1_win_count(y, d.s1_stride[g], Q.win, Q.win_max);
+        if (wc == 0) continue;
+        const i64 ncut = (i64)udiv(y, wc * Q.win) + 1;  // n >= ncut <=> q < wc*W
+        d.s1_wc[g] = wc;
+        d.s1_cnt[g] = ncut <= d.s1_n0[g] ? 0 : min(cnt, (ncut - 1 - d.s1_n0[g]) / d.s1_stride[g] + 1);
+    }
     u64 tot = (u64)d.s1_cnt[0] + (u64)d.s1_cnt[1];
     for (int p = 0; p < d.npieces; ++p) {
         d.mcnt[p] = piece_mcount(d.jlo[p], d.jhi[p]);

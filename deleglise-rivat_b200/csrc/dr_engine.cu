@@ -70,7 +70,7 @@ struct dr_ctx {
     // table buffers
     DevBuf dM, planes, ckpt, wheel, seg_sum, seg_off, primes, pinv, items, stencil;
     // query buffers
-    DevBuf queries, ops, prefix, scan_tmp, acc, counts, ticket, misc, inv, invw;
+    DevBuf queries, ops, prefix, scan_tmp, acc, counts, ticket, misc, inv, invw, wdesc, witems;
     // table state
     bool table_valid = false;
     int64_t t_u_total = 0, t_u_dense = 0, t_mu_limit = 0, t_nwords = 0;
@@ -88,6 +88,9 @@ struct dr_ctx {
     // owns its own staging, so replays never read memory a later call reuses)
     uint8_t* stage = nullptr;
     size_t stage_cap = 0, stage_used = 0;
+    // pinned copy of the windowed-S1 work items (single queries only, never captured)
+    S1WinItem* wstage = nullptr;
+    size_t wstage_cap = 0, wstage_used = 0;
     bool capturing = false;
     struct Graph {
         std::vector<int64_t> X;
@@ -409,6 +412,50 @@ int resolve_params(int64_t X, const dr_params* in, dr_params* out) {
     return dr_default_params(X, DR_POLICY_REFERENCE, out);
 }
 
+// Work items of the windowed S1 for one query (s1win_kernel): every window of W
+// values of the M table that some evaluation's windowed S1 lookups can reach, cut
+// into candidate ranges of about 2^21 lookups each.  Evaluation y takes window w iff
+// w < s1_win_count(y, stride) -- y >= DRB_WIN_MIN*W*(w+1)^2 at stride 1 -- and its S1
+// quotients start at cx*sqrt(y/2) - 1 or above, so the candidates whose y lies in
+// [DRB_WIN_MIN*W*(w+1)^2, 2*((w+1)*W + 4)^2/cx^2 + 16] cover the window (a superset: the
+// kernel finds each evaluation's exact divisor range).  The per-candidate work
+// falls like 1/k, so ranges are cut geometrically.
+std::vector<S1WinItem> s1win_items(const QueryDev& q, int qi) {
+    std::vector<S1WinItem> out;
+    if (q.win == 0 || q.nc <= 0) return out;
+    const double W = (double)q.win, X = (double)q.X;
+    const double target = 2097152.0;
+    for (uint64_t w = 0; w < q.win_max; ++w) {
+        const double ylo = (double)DRB_WIN_MIN * W * (double)(w + 1) * (double)(w + 1) * (1.0 - 1e-9) - 1.0;
+        const double yhi = 2.0 * std::pow(((double)(w + 1) * W + 4.0) / q.cx, 2.0) + 16.0;
+        if (ylo > X) break;  // larger windows need larger y still
+        const double klo = std::max(1.0, X / (3.0 * (yhi + 1.0)) - 1.0);
+        const double khi = std::min((double)q.N, X / ylo + 1.0);
+        if (klo > khi) continue;
+        const int64_t c0 = std::max<int64_t>(0, (int64_t)((klo - 2.0) / 3.0));
+        const int64_t c1 = std::min<int64_t>(q.nc, (int64_t)(khi / 3.0) + 1);
+        if (c0 >= c1) continue;
+        // lookups ~ sum over candidates of (4/3) * (X/k) * W / (2 Q^2), k ~ 3c + 1.5
+        const double Q = ((double)w + 0.5) * W;
+        const double K = X * W * (4.0 / 3.0) / (2.0 * 3.0 * Q * Q);
+        const double span = std::log(((double)c1 + 0.5) / ((double)c0 + 0.5));
+        const int64_t pieces = std::max<int64_t>(1, (int64_t)std::ceil(K * span / target));
+        const double r = std::exp(span / (double)pieces);
+        int64_t a = c0;
+        double edge = (double)c0 + 0.5;
+        for (int64_t i = 1; i <= pieces && a < c1; ++i) {
+            edge *= r;
+            int64_t b = i == pieces ? c1 : std::min<int64_t>(c1, std::max<int64_t>(a + 1, (int64_t)(edge - 0.5)));
+            while (a < b) {  // at most 2^15 candidates per item
+                const int64_t e = std::min<int64_t>(b, a + 32768);
+                out.push_back(S1WinItem{(uint32_t)w, (uint32_t)a, (uint32_t)e, (uint32_t)qi});
+                a = e;
+            }
+        }
+    }
+    return out;
+}
+
 // Enqueue planning and sums for a batch of queries on the current table.
 // Only stream operations: it can run under graph capture.
 int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, const dr_params* tuning,
@@ -433,6 +480,23 @@ int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq,
             inv_limit = std::max<int64_t>(inv_limit, (int64_t)std::min(b, 4.0e9));
         }
     }
+    // windowed S1: single queries (a batch keeps every lookup in the sums kernel)
+    std::vector<S1WinItem> witems;
+    for (int64_t i = 0; i < nq; ++i) {
+        QueryDev& q = qs[(size_t)i];
+        q.inv_limit = (u64)inv_limit;
+        q.win = q.win_max = 0;
+        // by default from X = 3e15 on (below it the direct S1 is as fast: measured)
+        if (P[i].s1_window_log2 == 0 && X[i] < 3000000000000000LL) continue;
+        const int wl = P[i].s1_window_log2 == 0 ? 15 : P[i].s1_window_log2;
+        if (nq != 1 || q.N <= 0 || wl < 12 || wl > 16) continue;
+        const int64_t W = int64_t(1) << wl;
+        q.win_max = (u64)(std::min<int64_t>(c->t_u_dense, (int64_t(1) << 31) - 1) / W);
+        if (q.win_max < 2) continue;
+        q.win = (u64)W;
+        witems = s1win_items(q, (int)i);
+        if (witems.empty()) q.win = q.win_max = 0;
+    }
     const int64_t invw_count = c->t_mu_limit / 6 + 1;  // every S2 j <= A <= mu_limit
     if ((rc = ensure(c, c->queries, (size_t)nq * sizeof(QueryDev)))) return rc;
     if ((rc = ensure(c, c->acc, (size_t)nq * 3 * 8))) return rc;
@@ -440,7 +504,11 @@ int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq,
     if ((rc = ensure(c, c->ops, (size_t)std::max<u64>(slots, 1) * 8))) return rc;
     if ((rc = ensure(c, c->prefix, (size_t)(slots + 1) * 8))) return rc;
     if ((rc = ensure(c, c->scan_tmp, scan_u64_tmp_elems(slots) * 8))) return rc;
-    if ((rc = ensure(c, c->ticket, 16))) return rc;
+    if ((rc = ensure(c, c->ticket, 32))) return rc;
+    if (!witems.empty()) {
+        if ((rc = ensure(c, c->wdesc, (size_t)std::max<u64>(slots, 1) * sizeof(S1WinDesc)))) return rc;
+        if ((rc = ensure(c, c->witems, witems.size() * sizeof(S1WinItem)))) return rc;
+    }
     if ((rc = ensure(c, c->inv, (size_t)(inv_limit + 1) * 8))) return rc;
     if ((rc = ensure(c, c->invw, (size_t)invw_count * 16))) return rc;
     const size_t need_pinned = (size_t)nq * 7 + 2;
@@ -454,26 +522,58 @@ int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq,
     }
     const void* sq = stage_put(c, qs.data(), (size_t)nq * sizeof(QueryDev));
     if (!sq) return fail(DR_ERR_NOMEM, "internal: staging area too small");
+    const void* sw = nullptr;
+    c->wstage_used = 0;
+    if (!witems.empty()) {
+        if (c->capturing) return fail(DR_ERR_ARG, "internal: windowed S1 under graph capture");
+        if (c->wstage_cap < witems.size()) {  // the previous call's copy has completed (it synchronised)
+            if (c->wstage) cudaFreeHost(c->wstage);
+            c->wstage = nullptr;
+            c->wstage_cap = 0;
+            const size_t cap = witems.size() + witems.size() / 4 + 1024;
+            CU(cudaMallocHost((void**)&c->wstage, cap * sizeof(S1WinItem)));
+            c->wstage_cap = cap;
+        }
+        std::memcpy(c->wstage, witems.data(), witems.size() * sizeof(S1WinItem));
+        c->wstage_used = witems.size() * sizeof(S1WinItem);
+        sw = c->wstage;
+    }
     const TableView T = view_of(c);
     const int qn = (int)nq;
     CU(record_event(c, 2));
     CU(cudaMemcpyAsync(c->queries.p, sq, (size_t)nq * sizeof(QueryDev), cudaMemcpyHostToDevice, c->stream));
     CU(cudaMemsetAsync(c->acc.p, 0, (size_t)nq * 3 * 8, c->stream));
     CU(cudaMemsetAsync(c->counts.p, 0, (size_t)nq * 4 * 8, c->stream));
-    CU(cudaMemsetAsync(c->ticket.p, 0, 16, c->stream));
+    CU(cudaMemsetAsync(c->ticket.p, 0, 32, c->stream));
+    if (sw)
+        CU(cudaMemcpyAsync(c->witems.p, sw, witems.size() * sizeof(S1WinItem), cudaMemcpyHostToDevice, c->stream));
     launch_direct((const QueryDev*)c->queries.p, qn, T, (u64*)c->acc.p, c->stream);
     int launches = 1;
     if (slots > 0) {
         launch_inverse((double*)c->inv.p, inv_limit, (double2*)c->invw.p, invw_count, T.wheel, c->sm_count,
                        c->stream);
         launch_plan((const QueryDev*)c->queries.p, qn, T, slots, (u64*)c->ops.p, (u64*)c->acc.p, (i64*)c->counts.p,
-                    c->sm_count, c->stream);
+                    sw ? (S1WinDesc*)c->wdesc.p : nullptr, c->sm_count, c->stream);
         launch_scan_u64((const u64*)c->ops.p, (u64*)c->prefix.p, slots, (u64*)c->scan_tmp.p,
                         scan_u64_tmp_elems(slots), c->stream);
         launches += 5;
     }
     CU(cudaGetLastError());
     CU(record_event(c, 3));
+    if (slots > 0 && sw) {
+        S1WinArgs wa;
+        wa.items = (const S1WinItem*)c->witems.p;
+        wa.n_items = witems.size();
+        wa.desc = (const S1WinDesc*)c->wdesc.p;
+        wa.queries = (const QueryDev*)c->queries.p;
+        wa.T = T;
+        wa.rcp = (const double*)c->inv.p;
+        wa.ticket = (u64*)c->ticket.p + 2;
+        wa.acc = (u64*)c->acc.p;
+        launch_s1win(wa, qs[0].win, c->sm_count, c->stream);
+        CU(cudaGetLastError());
+        launches += 1;
+    }
     if (slots > 0) {
         SumsArgs sa;
         sa.queries = (const QueryDev*)c->queries.p;
@@ -670,11 +770,12 @@ int dr_ctx_destroy(dr_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     DevBuf* bufs[] = {&c->dM, &c->planes, &c->ckpt, &c->wheel, &c->seg_sum, &c->seg_off, &c->primes, &c->pinv, &c->items, &c->stencil,
                       &c->queries, &c->ops, &c->prefix, &c->scan_tmp, &c->acc, &c->counts, &c->ticket, &c->misc,
-                      &c->inv, &c->invw};
+                      &c->inv, &c->invw, &c->wdesc, &c->witems};
     for (DevBuf* b : bufs) release(c, *b);
     drop_graphs(c);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->stage) cudaFreeHost(c->stage);
+    if (c->wstage) cudaFreeHost(c->wstage);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -832,7 +933,7 @@ int dr_mertens_batch(dr_ctx* c, const int64_t* X, int64_t count, const dr_params
     int launches = 0;
     rc = enqueue_queries(c, X, P.data(), count, &tune, &launches);
     if (rc) return rc;
-    rc = finish_queries(c, X, count, launches, c->stage_used, out, st);
+    rc = finish_queries(c, X, count, launches, c->stage_used + c->wstage_used, out, st);
     if (rc) return rc;
     if (st) st->total_ms = now_ms() - t0;
     if (count > 1 && c->graphs_enabled) capture_graph(c, X, P.data(), count, tune, ut, ud, ml, n_primes);

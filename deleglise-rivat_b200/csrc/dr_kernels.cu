@@ -383,7 +383,8 @@ __device__ __forceinline__ int query_of_slot(const QueryDev* q, int nq, u64 s) {
 
 // counts[4*q + 0..3]: terms, evaluations, S1 lookups, S2 wheel positions
 __global__ void plan_kernel(const QueryDev* __restrict__ qs, int nq, const TableView T, u64 n_slots,
-                            u64* __restrict__ ops, u64* __restrict__ acc, i64* __restrict__ counts) {
+                            u64* __restrict__ ops, u64* __restrict__ acc, i64* __restrict__ counts,
+                            S1WinDesc* __restrict__ wdesc) {
     const u64 stride = (u64)gridDim.x * blockDim.x;
     for (u64 s = (u64)blockIdx.x * blockDim.x + threadIdx.x; s < n_slots; s += stride) {
         const int qi = query_of_slot(qs, nq, s);
@@ -392,24 +393,39 @@ __global__ void plan_kernel(const QueryDev* __restrict__ qs, int nq, const Table
         EvalDesc d;
         decode_eval(Q, T, (i64)(local >> 1), (int)(local & 1), d);
         ops[s] = d.total;
+        if (wdesc && Q.win) {
+            S1WinDesc w;
+            w.y = d.y;
+            for (int g = 0; g < 2; ++g) {
+                const bool on = d.kind != EVAL_NONE && d.s1_full[g] > 0 && d.s1_wc[g] > 0;
+                w.n0[g] = on ? (uint32_t)d.s1_n0[g] : 0u;
+                w.cnt[g] = on ? (uint32_t)d.s1_full[g] : 0u;
+                w.wc[g] = on ? (uint32_t)d.s1_wc[g] : 0u;
+                w.w0[g] = on ? (uint32_t)(udiv(d.y, (u64)(d.s1_n0[g] + (i64)d.s1_stride[g] * (d.s1_full[g] - 1))) /
+                                          Q.win)
+                             : 0u;
+                w.sg[g] = on ? (int32_t)(d.coef * d.s1_sign[g]) * d.s1_stride[g] : 0;
+            }
+            wdesc[s] = w;
+        }
         if (d.kind != EVAL_NONE) {
             const i64 c = d.coef * eval_constant(d, T);
             atomicAdd(acc + 3 * qi, (u64)c);
             unsigned long long* cq = reinterpret_cast<unsigned long long*>(counts + 4 * qi);
             if ((local & 1) == 0) atomicAdd(cq + 0, 1ull);
             atomicAdd(cq + 1, 1ull);
-            const u64 s1n = (u64)d.s1_cnt[0] + (u64)d.s1_cnt[1];
-            atomicAdd(cq + 2, s1n);
-            atomicAdd(cq + 3, d.total - s1n);
+            const u64 s1d = (u64)d.s1_cnt[0] + (u64)d.s1_cnt[1];  // left to the sums kernel
+            atomicAdd(cq + 2, (u64)d.s1_full[0] + (u64)d.s1_full[1]);
+            atomicAdd(cq + 3, d.total - s1d);
         }
     }
 }
 
 void launch_plan(const QueryDev* q, int nq, const TableView& T, u64 n_slots, u64* ops, u64* acc, i64* counts,
-                 int sm_count, cudaStream_t s) {
+                 S1WinDesc* wdesc, int sm_count, cudaStream_t s) {
     if (n_slots == 0) return;
     const int grid = (int)std::min<u64>((n_slots + 127) / 128, (u64)sm_count * 16);
-    plan_kernel<<<grid, 128, 0, s>>>(q, nq, T, n_slots, ops, acc, counts);
+    plan_kernel<<<grid, 128, 0, s>>>(q, nq, T, n_slots, ops, acc, counts, wdesc);
 }
 
 // Direct answers for queries with X <= table u_total (get_M, :1465-1467).
@@ -894,6 +910,136 @@ __global__ void __launch_bounds__(256, DRB_SUMS_MINB) sums_kernel(const SumsArgs
             atomicAdd(a.acc + 3 * cur_q + 2, t2);
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Windowed S1.  Each work item is one window of the M table, q in [w*W, (w+1)*W),
+// and a range of evaluation candidates: the CTA stages M(w*W - 7 .. (w+1)*W), i.e.
+// dM[w*W - 8 .. (w+1)*W - 1], in shared memory (16-byte loads; window 0 element by
+// element, M(0) = 0), and its warps sum, candidate by candidate, every
+// windowed S1 lookup M(floor(y/n)) whose quotient falls in the window: for each
+// S1 segment the divisors n in (y/((w+1)W), y/(wW)] -- two exact quotients per
+// evaluation and window -- with lanes on consecutive n.  Each lookup is one
+// reciprocal load, the 32-bit quotient route and one shared-memory read, so the M
+// gathers no longer cross L2.  The lookups with q above a segment's windows are
+// the sums kernel's (decode_eval); together they are every S1 lookup exactly once.
+// ---------------------------------------------------------------------------
+constexpr int kWinThreads = 512;
+
+// sum of M(q) over n = na + st*i, i < cnt, q in the window [qbase, qbase + W) (qbase a
+// multiple of W, so q - qbase = q & (W - 1)); lanes take consecutive n.  The
+// reciprocal loads mostly hit L1 (neighbouring windows reuse the same divisors).
+__device__ __forceinline__ int32_t s1win_range(const int16_t* win, uint32_t wmask, const double* rcp, double yd,
+                                               uint32_t ylo, uint32_t na, uint32_t st, uint32_t cnt, int lane) {
+    int32_t part = 0;
+    const int16_t* w7 = win + 7;
+    uint32_t i = (uint32_t)lane;
+    for (; i + 96u < cnt; i += 128u) {
+        uint32_t n[4];
+        double r[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            n[k] = na + st * (i + 32u * k);
+            r[k] = __ldg(rcp + n[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) part += w7[qfix(qest(yd, r[k]), ylo, n[k]) & wmask];
+    }
+    for (; i < cnt; i += 32u) {
+        const uint32_t nn = na + st * i;
+        part += w7[qfix(qest(yd, __ldg(rcp + nn)), ylo, nn) & wmask];
+    }
+    return part;
+}
+
+__global__ void __launch_bounds__(kWinThreads, 2) s1win_kernel(const S1WinArgs a, uint32_t W) {
+    extern __shared__ __align__(16) int16_t win[];  // win[7 + i] = M(w*W + i), i < W
+    __shared__ S1WinItem it;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t wmask = W - 1u;
+    uint32_t cur = 0xFFFFFFFFu;
+    int cur_q = -1;
+    i64 acc = 0;
+    for (;;) {
+        __syncthreads();  // the previous item's readers are done with `it` and the window
+        if (threadIdx.x == 0) {
+            const u64 t = atomicAdd(a.ticket, 1ull);
+            it = t < a.n_items ? a.items[t] : S1WinItem{0xFFFFFFFFu, 0u, 0u, 0u};
+        }
+        __syncthreads();
+        const S1WinItem I = it;
+        if (I.w == 0xFFFFFFFFu) break;
+        if ((int)I.q != cur_q) {
+            if (cur_q >= 0) {
+                const u64 t = warp_sum_u64((u64)acc);
+                if (lane == 0) atomicAdd(a.acc + 3 * cur_q + 1, t);
+            }
+            acc = 0;
+            cur_q = (int)I.q;
+            cur = 0xFFFFFFFFu;
+        }
+        if (I.w != cur) {  // stage the window: win[t] = M(w*W - 7 + t) = dM[w*W - 8 + t], t < W + 8
+            if (I.w > 0) {
+                const uint4* src = reinterpret_cast<const uint4*>(a.T.dM + ((u64)I.w * W - 8));
+                uint4* dst = reinterpret_cast<uint4*>(win);
+                for (uint32_t t = threadIdx.x; t < (W + 8u) / 8u; t += blockDim.x) dst[t] = __ldg(src + t);
+            } else {
+                for (uint32_t t = threadIdx.x; t < W + 8u; t += blockDim.x)
+                    win[t] = t >= 8u ? __ldg(a.T.dM + (t - 8u)) : (int16_t)0;
+            }
+            cur = I.w;
+            __syncthreads();
+        }
+        const QueryDev Q = a.queries[I.q];
+        const u64 qlo = (u64)I.w * W, qhi = qlo + W;  // window: q in [qlo, qhi)
+        const double rlo = qlo ? __drcp_rn((double)qlo) : 0.0, rhi = __drcp_rn((double)qhi);
+        for (uint32_t c = I.c0 + (uint32_t)warp; c < I.c1; c += (uint32_t)nwarps) {
+#pragma unroll 1
+            for (int e = 0; e < 2; ++e) {
+                const S1WinDesc D = a.desc[Q.slot_base + 2ull * c + (u64)e];
+                const bool on0 = D.cnt[0] && D.w0[0] <= I.w && I.w < D.wc[0];
+                const bool on1 = D.cnt[1] && D.w0[1] <= I.w && I.w < D.wc[1];
+                if (!(on0 || on1)) continue;
+                const double yd = __ull2double_rn(D.y);
+                // n in (y/qhi, y/qlo]  <=>  floor(y/n) in [qlo, qhi)
+                // exact quotients: udiv_rcp while y/q < 2^50 (q < 2^31 here), else udiv
+                const u64 nlo = ((D.y >> 50) < qhi ? udiv_rcp(D.y, yd, (uint32_t)qhi, rhi) : udiv(D.y, qhi)) + 1;
+                const u64 nhi = qlo == 0 ? ~0ull
+                                         : (D.y >> 50) < qlo ? udiv_rcp(D.y, yd, (uint32_t)qlo, rlo) : udiv(D.y, qlo);
+#pragma unroll 1
+                for (int g = 0; g < 2; ++g) {
+                    if (!(g == 0 ? on0 : on1)) continue;
+                    const uint32_t st = (uint32_t)(D.sg[g] < 0 ? -D.sg[g] : D.sg[g]);
+                    const u64 n0 = D.n0[g], nend = n0 + (u64)st * (D.cnt[g] - 1);
+                    u64 na = max(n0, nlo);
+                    if (st == 2) na += (na - n0) & 1;  // strides are 1 or 2
+                    const u64 nb = min(nend, nhi);
+                    if (na > nb) continue;
+                    const uint32_t cnt = (uint32_t)((nb - na) / st + 1);
+                    const int32_t part = s1win_range(win, wmask, a.rcp, yd, (uint32_t)D.y, (uint32_t)na, st, cnt, lane);
+                    acc += D.sg[g] > 0 ? (i64)part : -(i64)part;
+                }
+            }
+        }
+    }
+    if (cur_q >= 0) {
+        const u64 t = warp_sum_u64((u64)acc);
+        if (lane == 0) atomicAdd(a.acc + 3 * cur_q + 1, t);
+    }
+}
+
+void launch_s1win(const S1WinArgs& a, u64 win, int sm_count, cudaStream_t s) {
+    if (a.n_items == 0) return;
+    const size_t smem = (size_t)(win + 8) * 2;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(s1win_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(((1u << 16) + 8) * 2));
+        attr = true;
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, s1win_kernel, kWinThreads, smem);
+    const int grid = sm_count * std::max(1, per_sm);
+    s1win_kernel<<<grid, kWinThreads, smem, s>>>(a, (uint32_t)win);
 }
 
 // rcp[n] = RN(1/n) for 1 <= n <= inv_limit.  invw[m] = {rcp(6m+1), rcp(6m+5)} with

@@ -33,6 +33,34 @@ struct SieveArgs {
     int32_t* seg_sum;
 };
 
+// One evaluation as seen by s1win_kernel (written by plan_kernel): its two S1
+// segments n = n0 + |sg|*i, i < cnt, with sign sg/|sg| (mu(k) times the segment's
+// sign), and the windows [w0, wc) in which each segment has windowed lookups.
+struct S1WinDesc {
+    u64 y;
+    uint32_t n0[2];
+    uint32_t cnt[2];
+    uint32_t w0[2];  // first window holding a lookup: floor(y / n_last) / W
+    uint32_t wc[2];
+    int32_t sg[2];   // +-stride; 0: no S1 segment
+};
+
+// Work item of s1win_kernel: window w of query q, evaluation candidates [c0, c1).
+struct S1WinItem {
+    uint32_t w, c0, c1, q;
+};
+
+struct S1WinArgs {
+    const S1WinItem* items;
+    u64 n_items;
+    const S1WinDesc* desc;  // per evaluation slot
+    const QueryDev* queries;
+    TableView T;
+    const double* rcp;      // RN(1/n), n <= inv_limit
+    u64* ticket;            // work-queue counter, zeroed before launch
+    u64* acc;               // [3 * nq]: C, S1, S2
+};
+
 struct SumsArgs {
     const QueryDev* queries;
     int nq;
@@ -65,7 +93,9 @@ void launch_seg_scan(const int32_t* in, int32_t* out, i64 n, cudaStream_t s);
 void launch_fixup(int16_t* dM, i64 u_dense, int S, const int32_t* seg_off, int32_t* ckpt, i64 nwords,
                   i64 dense_segs, int sm_count, cudaStream_t s);
 void launch_plan(const QueryDev* q, int nq, const TableView& T, u64 n_slots, u64* ops, u64* acc,
-                 i64* counts, int sm_count, cudaStream_t s);
+                 i64* counts, S1WinDesc* wdesc, int sm_count, cudaStream_t s);
+// Windowed S1 (window length win: a power of two, 2^12 .. 2^16).
+void launch_s1win(const S1WinArgs& a, u64 win, int sm_count, cudaStream_t s);
 void launch_scan_u64(const u64* in, u64* out, u64 n, u64* tmp, size_t tmp_elems, cudaStream_t s);
 size_t scan_u64_tmp_elems(u64 n);
 void launch_sums(const SumsArgs& a, int grid, int block, cudaStream_t s);

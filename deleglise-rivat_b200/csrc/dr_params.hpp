@@ -93,7 +93,7 @@ inline bool ref_use_compressed(int64_t X) {
 inline void params_clear(dr_params* p) {
     p->u_total = p->u_dense = p->mu_limit = 0;
     p->cx = 0.0;
-    p->segment_log2 = p->block_threads = p->chunk_log2 = p->reserved = 0;
+    p->segment_log2 = p->block_threads = p->chunk_log2 = p->s1_window_log2 = 0;
 }
 
 // Dense path parameters (mertens_dr.hpp:1033-1041 with SieveTable's clamp :396).

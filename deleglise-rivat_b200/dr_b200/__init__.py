@@ -50,11 +50,11 @@ class Params(ctypes.Structure):
         ("segment_log2", ctypes.c_int32),
         ("block_threads", ctypes.c_int32),
         ("chunk_log2", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("s1_window_log2", ctypes.c_int32),
     ]
 
     def as_dict(self) -> dict:
-        return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
     def __repr__(self) -> str:
         return f"Params({self.as_dict()})"

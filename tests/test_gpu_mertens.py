@@ -107,3 +107,25 @@ def test_m1e18(engine):
     r = engine.mertens(g["X"], p)
     assert r.M == g["M"]
     assert (r.stats.C - r.stats.S1 - r.stats.S2) % (1 << 64) == g["M"] % (1 << 64)
+
+
+def test_windowed_s1_matches_direct(engine):
+    """The windowed S1 (s1win_kernel) and the sums kernel's direct S1 split every S1
+    lookup between them; with the window switched off the sums kernel takes them
+    all.  Both give the same M(X), the same C/S1/S2 checksums and the same S1 op
+    count, for every window length and for inputs that reach window 0."""
+    cases = [(10**9 + 7, 12), (2 * 10**10 + 1, 13), (10**11, 14), (3 * 10**12, 15), (10**14, 16), (10**15, 15),
+             (10**16, 0)]
+    for X, wl in cases:
+        p = dr_b200.default_params(X, dr_b200.POLICY_GPU)
+        on = dr_b200.Params(**{**p.as_dict(), "s1_window_log2": wl})
+        off = dr_b200.Params(**{**p.as_dict(), "s1_window_log2": -1})
+        r1, r0 = engine.mertens(X, on), engine.mertens(X, off)
+        got = (r1.M, r1.stats.C, r1.stats.S1, r1.stats.S2, r1.stats.s1_ops, r1.stats.s2_ops)
+        want = (r0.M, r0.stats.C, r0.stats.S1, r0.stats.S2, r0.stats.s1_ops, r0.stats.s2_ops)
+        assert got == want, (X, wl)
+    # a dense tier smaller than two windows switches the windowed S1 off by itself
+    X = 10**12
+    p = dr_b200.default_params(X, dr_b200.POLICY_GPU)
+    small = dr_b200.Params(**{**p.as_dict(), "u_dense": 40000, "s1_window_log2": 15})
+    assert engine.mertens(X, small).M == 62366
