@@ -68,7 +68,8 @@ struct dr_ctx {
     uint64_t budget = 0;
     uint64_t held = 0;
     // table buffers
-    DevBuf dM, planes, ckpt, wheel, seg_sum, seg_off, primes, pinv, items, stencil;
+    DevBuf dM, planes, ckpt, wheel, seg_sum, seg_off, primes, pinv, items, stencil, prcp;
+    DevBuf sq_cnt, sq_off, sq_cur, sq_pos, sq_tmp;  // bucketed square hits per segment
     // query buffers
     DevBuf queries, ops, prefix, scan_tmp, acc, counts, ticket, misc, inv, invw, wdesc, witems;
     // table state
@@ -78,6 +79,7 @@ struct dr_ctx {
     // host
     std::vector<uint32_t> host_primes;
     std::vector<uint64_t> host_pinv;  // per prime: floor((2^64-1)/p), then floor((2^64-1)/p^2)
+    std::vector<double> host_prcp;    // per prime: RN(1/p)
     int64_t host_primes_root = -1;
     uint64_t* pinned = nullptr;  // 3 * pinned_q u64 + counts
     size_t pinned_cap = 0;
@@ -196,7 +198,7 @@ const void* stage_put(dr_ctx* c, const void* src, size_t bytes) {
 }
 
 size_t stage_bytes_for(size_t n_primes, int64_t nq) {
-    return n_primes * 20 + (size_t)kMaxSieveItems * 16 + (size_t)nq * sizeof(QueryDev) + 256;
+    return n_primes * 28 + (size_t)kMaxSieveItems * 16 + (size_t)nq * sizeof(QueryDev) + 256;
 }
 
 // Sieving primes up to root, cached per context.
@@ -314,12 +316,19 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     const std::vector<uint32_t>& pr = primes_upto(c, isqrt_i64(u_total));
     if ((rc = ensure(c, c->primes, pr.size() * 4))) return rc;
     if ((rc = ensure(c, c->pinv, pr.size() * 16))) return rc;
+    if ((rc = ensure(c, c->prcp, pr.size() * 8))) return rc;
+    if (c->host_prcp.size() != pr.size()) {
+        c->host_prcp.resize(pr.size());
+        for (size_t i = 0; i < pr.size(); ++i) c->host_prcp[i] = 1.0 / (double)pr[i];  // IEEE: RN(1/p)
+    }
     if (!pr.empty()) {
         const void* sp = stage_put(c, pr.data(), pr.size() * 4);
         const void* sv = stage_put(c, c->host_pinv.data(), pr.size() * 16);
-        if (!sp || !sv) return fail(DR_ERR_NOMEM, "internal: staging area too small");
+        const void* sr = stage_put(c, c->host_prcp.data(), pr.size() * 8);
+        if (!sp || !sv || !sr) return fail(DR_ERR_NOMEM, "internal: staging area too small");
         CU(cudaMemcpyAsync(c->primes.p, sp, pr.size() * 4, cudaMemcpyHostToDevice, c->stream));
         CU(cudaMemcpyAsync(c->pinv.p, sv, pr.size() * 16, cudaMemcpyHostToDevice, c->stream));
+        CU(cudaMemcpyAsync(c->prcp.p, sr, pr.size() * 8, cudaMemcpyHostToDevice, c->stream));
     }
 
     SieveArgs a;
@@ -354,6 +363,26 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     a.primes = (const uint32_t*)c->primes.p;
     a.pinv = (const u64*)c->pinv.p;
     a.sqinv = (const u64*)c->pinv.p + pr.size();
+    a.prcp = (const double*)c->prcp.p;
+    // squares above S hit a segment at most once: bucket their hits per segment
+    // (sizes known here exactly: sum of floor(u_total / p^2) over those primes)
+    int lgS = 0;
+    while ((1 << lgS) < S) ++lgS;
+    a.sqC_first = a.sqB_first;
+    while (a.sqC_first < (int)pr.size() && (uint64_t)pr[a.sqC_first] * pr[a.sqC_first] <= (uint64_t)S) ++a.sqC_first;
+    uint64_t sq_hits = 0;
+    for (size_t i = (size_t)a.sqC_first; i < pr.size(); ++i) sq_hits += (uint64_t)u_total / ((uint64_t)pr[i] * pr[i]);
+    a.sq_off = nullptr;
+    a.sq_pos = nullptr;
+    if (sq_hits > 0) {
+        if ((rc = ensure(c, c->sq_cnt, (size_t)nseg * 8))) return rc;
+        if ((rc = ensure(c, c->sq_cur, (size_t)nseg * 8))) return rc;
+        if ((rc = ensure(c, c->sq_off, (size_t)(nseg + 1) * 8))) return rc;
+        if ((rc = ensure(c, c->sq_tmp, scan_u64_tmp_elems((u64)nseg) * 8))) return rc;
+        if ((rc = ensure(c, c->sq_pos, (size_t)sq_hits * 4))) return rc;
+        a.sq_off = (const u64*)c->sq_off.p;
+        a.sq_pos = (const uint32_t*)c->sq_pos.p;
+    }
     a.stencil4 = (const uint32_t*)c->stencil.p;
     a.dM = (int16_t*)c->dM.p;
     a.planes = (ulonglong2*)c->planes.p;
@@ -369,6 +398,19 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
 
     CU(record_event(c, 0));
     CU(cudaMemsetAsync(c->wheel.p, 0, (size_t)wheel_groups * 16, c->stream));
+    int launches = 3;
+    if (a.sq_off) {
+        CU(cudaMemsetAsync(c->sq_cnt.p, 0, (size_t)nseg * 8, c->stream));
+        CU(cudaMemsetAsync(c->sq_cur.p, 0, (size_t)nseg * 8, c->stream));
+        launch_sq_bucket_count((const uint32_t*)c->primes.p, a.sqC_first, (int)pr.size(), u_total, u_dense, dense_segs,
+                               lgS, (u64*)c->sq_cnt.p, c->stream);
+        launch_scan_u64((const u64*)c->sq_cnt.p, (u64*)c->sq_off.p, (u64)nseg, (u64*)c->sq_tmp.p,
+                        scan_u64_tmp_elems((u64)nseg), c->stream);
+        launch_sq_bucket_fill((const uint32_t*)c->primes.p, a.sqC_first, (int)pr.size(), u_total, u_dense, dense_segs,
+                              lgS, (const u64*)c->sq_off.p, (u64*)c->sq_cur.p, (uint32_t*)c->sq_pos.p, c->stream);
+        CU(cudaGetLastError());
+        launches += 5;
+    }
     launch_sieve(a, grid, block, smem, c->stream);
     CU(cudaGetLastError());
     launch_seg_scan((const int32_t*)c->seg_sum.p, (int32_t*)c->seg_off.p, nseg, c->stream);
@@ -384,7 +426,7 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     c->t_mu_limit = mu_limit;
     c->t_nwords = nwords;
     c->t_S = S;
-    if (st) st->kernel_launches += 3;
+    if (st) st->kernel_launches += launches;
     return DR_OK;
 }
 
@@ -417,14 +459,45 @@ int resolve_params(int64_t X, const dr_params* in, dr_params* out) {
 // into candidate ranges of about 2^21 lookups each.  Evaluation y takes window w iff
 // w < s1_win_count(y, stride) -- y >= DRB_WIN_MIN*W*(w+1)^2 at stride 1 -- and its S1
 // quotients start at cx*sqrt(y/2) - 1 or above, so the candidates whose y lies in
-// [DRB_WIN_MIN*W*(w+1)^2, 2*((w+1)*W + 4)^2/cx^2 + 16] cover the window (a superset: the
-// kernel finds each evaluation's exact divisor range).  The per-candidate work
-// falls like 1/k, so ranges are cut geometrically.
+// [DRB_WIN_MIN*W*(w+1)^2, 2*((w+1)*W + 4)^2/cx^2 + 16] cover the window (a superset:
+// the kernel finds each evaluation's exact divisor range).  A candidate's work in the
+// window is estimated from the overlap of its divisor range (n <= sqrt(2y)/cx or
+// sqrt(y)/cx) with (y/((w+1)W), y/(wW)], sampled at geometric points of the
+// candidate range and integrated; the cuts follow that estimate.
+namespace {
+
+double s1win_est(double y, int stride, uint64_t w, double W, double cx) {
+    const double wc = std::floor(std::sqrt(y * W / ((double)DRB_WIN_MIN * stride)) / W);
+    if ((double)w >= wc) return 0.0;
+    const double nmax = (stride == 2 ? std::sqrt(2.0 * y) : std::sqrt(y)) / cx;
+    const double hi = w ? std::min(y / ((double)w * W), nmax) : nmax;
+    const double lo = y / ((double)(w + 1) * W);
+    return hi > lo ? (hi - lo) / stride : 0.0;
+}
+
+// estimated windowed lookups of candidate c (both evaluations) in window w
+double s1win_cand_est(int64_t c, uint64_t w, double W, const QueryDev& q) {
+    const int64_t k = 3 * c + 1 + (c & 1);
+    if (k > q.N) return 0.0;
+    const int64_t N = q.N;
+    const int range = k <= N / 6 ? 1 : k <= N / 3 ? 2 : k <= N / 2 ? 3 : 4;
+    const double y = (double)q.X / (double)k;
+    double t = s1win_est(y, range <= 3 ? 2 : 1, w, W, q.cx);
+    if (range == 1) t += s1win_est(y / 3.0, 2, w, W, q.cx);
+    else if (range == 2) t += s1win_est(y / 3.0, 1, w, W, q.cx);
+    return t;
+}
+
+}  // namespace
+
 std::vector<S1WinItem> s1win_items(const QueryDev& q, int qi) {
     std::vector<S1WinItem> out;
     if (q.win == 0 || q.nc <= 0) return out;
     const double W = (double)q.win, X = (double)q.X;
     const double target = 2097152.0;
+    constexpr int kSamples = 32;
+    std::vector<int64_t> edge;
+    std::vector<double> cum;
     for (uint64_t w = 0; w < q.win_max; ++w) {
         const double ylo = (double)DRB_WIN_MIN * W * (double)(w + 1) * (double)(w + 1) * (1.0 - 1e-9) - 1.0;
         const double yhi = 2.0 * std::pow(((double)(w + 1) * W + 4.0) / q.cx, 2.0) + 16.0;
@@ -435,17 +508,33 @@ std::vector<S1WinItem> s1win_items(const QueryDev& q, int qi) {
         const int64_t c0 = std::max<int64_t>(0, (int64_t)((klo - 2.0) / 3.0));
         const int64_t c1 = std::min<int64_t>(q.nc, (int64_t)(khi / 3.0) + 1);
         if (c0 >= c1) continue;
-        // lookups ~ sum over candidates of (4/3) * (X/k) * W / (2 Q^2), k ~ 3c + 1.5
-        const double Q = ((double)w + 0.5) * W;
-        const double K = X * W * (4.0 / 3.0) / (2.0 * 3.0 * Q * Q);
-        const double span = std::log(((double)c1 + 0.5) / ((double)c0 + 0.5));
-        const int64_t pieces = std::max<int64_t>(1, (int64_t)std::ceil(K * span / target));
-        const double r = std::exp(span / (double)pieces);
+        // geometric sample edges c0 .. c1 and the integrated estimate up to each
+        edge.assign(1, c0);
+        for (int j = 1; j <= kSamples; ++j) {
+            const int64_t e = j == kSamples ? c1
+                                            : c0 + (int64_t)std::llround(std::pow((double)(c1 - c0), (double)j / kSamples)) - 1;
+            if (e > edge.back() && e <= c1) edge.push_back(e);
+        }
+        if (edge.back() != c1) edge.push_back(c1);
+        cum.assign(1, 0.0);
+        for (size_t j = 1; j < edge.size(); ++j) {
+            const double ga = s1win_cand_est(edge[j - 1], w, W, q), gb = s1win_cand_est(edge[j] - 1, w, W, q);
+            cum.push_back(cum.back() + 0.5 * (ga + gb) * (double)(edge[j] - edge[j - 1]));
+        }
+        const double total = cum.back();
+        // a window whose estimate is 0 may still hold a few lookups: one item
+        const int64_t pieces = std::max<int64_t>(1, (int64_t)std::ceil(total / target));
         int64_t a = c0;
-        double edge = (double)c0 + 0.5;
-        for (int64_t i = 1; i <= pieces && a < c1; ++i) {
-            edge *= r;
-            int64_t b = i == pieces ? c1 : std::min<int64_t>(c1, std::max<int64_t>(a + 1, (int64_t)(edge - 0.5)));
+        size_t j = 1;
+        for (int64_t i = 1; i <= pieces; ++i) {
+            int64_t b = c1;
+            if (i < pieces) {
+                const double t = total * (double)i / (double)pieces;
+                while (j + 1 < cum.size() && cum[j] < t) ++j;
+                const double span = cum[j] - cum[j - 1];
+                const double f = span > 0.0 ? (t - cum[j - 1]) / span : 1.0;
+                b = std::min(c1, std::max(a, edge[j - 1] + (int64_t)(f * (double)(edge[j] - edge[j - 1]))));
+            }
             while (a < b) {  // at most 2^15 candidates per item
                 const int64_t e = std::min<int64_t>(b, a + 32768);
                 out.push_back(S1WinItem{(uint32_t)w, (uint32_t)a, (uint32_t)e, (uint32_t)qi});
@@ -770,7 +859,8 @@ int dr_ctx_destroy(dr_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     DevBuf* bufs[] = {&c->dM, &c->planes, &c->ckpt, &c->wheel, &c->seg_sum, &c->seg_off, &c->primes, &c->pinv, &c->items, &c->stencil,
                       &c->queries, &c->ops, &c->prefix, &c->scan_tmp, &c->acc, &c->counts, &c->ticket, &c->misc,
-                      &c->inv, &c->invw, &c->wdesc, &c->witems};
+                      &c->inv, &c->invw, &c->wdesc, &c->witems, &c->prcp, &c->sq_cnt, &c->sq_off, &c->sq_cur,
+                      &c->sq_pos, &c->sq_tmp};
     for (DevBuf* b : bufs) release(c, *b);
     drop_graphs(c);
     if (c->pinned) cudaFreeHost(c->pinned);
@@ -823,7 +913,10 @@ uint64_t dr_table_bytes(int64_t u_total, int64_t u_dense, int64_t mu_limit) {
     const int64_t comp = std::max<int64_t>(0, u_total - u_dense);
     const int64_t nwords = (comp + 63) / 64;
     const int64_t nseg = (u_total + 4095) / 4096 + 2;
-    return (uint64_t)u_dense * 2 + (uint64_t)nwords * 20 + (uint64_t)(mu_limit / 192 + 2) * 16 + (uint64_t)nseg * 8;
+    // + bucketed square hits: u * sum over primes p^2 > S of 1/p^2 < u / (sqrt(S) ln sqrt(S)),
+    // 4 bytes each, for the default S = 2^17 (at most 0.0019 u bytes)
+    return (uint64_t)u_dense * 2 + (uint64_t)nwords * 20 + (uint64_t)(mu_limit / 192 + 2) * 16 + (uint64_t)nseg * 32 +
+           (uint64_t)u_total / 500;
 }
 
 uint64_t dr_query_bytes(int64_t X, const dr_params* p) {

@@ -155,7 +155,10 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
             }
         }
         //    Larger moduli (at most 32 hits per segment): one prime per thread.
-        for (int i = a.sqB_first + tid; i < a.n_primes; i += T) {
+        //    Squares above S hit a segment at most once: their hits come from
+        //    the per-segment bucket (sq_off / sq_pos) when there is one.
+        const int sq_end = a.sq_off ? a.sqC_first : a.n_primes;
+        for (int i = a.sqB_first + tid; i < sq_end; i += T) {
             const u64 p = a.primes[i];
             const u64 sq = p * p;
             if (sq > (u64)end) break;
@@ -163,37 +166,63 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
             for (u64 j = r ? sq - r : 0; j < (u64)len; j += sq)
                 atomicOr(&buf32[j >> 2], 0x80u << ((j & 3) * 8));
         }
+        if (a.sq_off) {
+            const u64 h1 = __ldg(a.sq_off + seg + 1);
+            for (u64 h = __ldg(a.sq_off + seg) + tid; h < h1; h += T) {
+                const uint32_t j = __ldg(a.sq_pos + h);
+                atomicOr(&buf32[j >> 2], 0x80u << ((j & 3) * 8));
+            }
+        }
+        //    Offsets low mod p: on the 32-bit quotient route (qest/qfix) while
+        //    p <= low and low/p < 2^31, else from the 64-bit reciprocal.
+        const double lowd = __ull2double_rn((u64)low);
         for (int i = a.tierB_first + tid; i < a.n_primes; i += T) {
             const uint32_t p = a.primes[i];
             const uint32_t w = (32u - __clz(p - 1)) | 1u;
-            const uint32_t r = (uint32_t)umod_inv((u64)low, p, a.pinv[i]);
+            uint32_t r;
+            if (a.prcp && (u64)low >= p && ((u64)low >> 31) < p)
+                r = (uint32_t)low - qfix(qest(lowd, __ldg(a.prcp + i)), (uint32_t)low, p) * p;
+            else
+                r = (uint32_t)umod_inv((u64)low, p, a.pinv[i]);
             for (uint32_t j = r ? p - r : 0; j < (uint32_t)len; j += p)
                 atomicAdd(&buf32[j >> 2], w << ((j & 3) * 8));
         }
         __syncthreads();
 
-        // 4. finalize to mu bytes in place, four at a time with byte-SIMD
-        //    compares (all four share floor(log2 n) unless the word straddles a
-        //    power of two); bytes past len become 0
-        for (int i = tid; i < nw16; i += T) {
-            const uint32_t v = buf32[i];
-            const u64 n0 = (u64)(low + 4 * i);
-            uint32_t o;
-            const int bw0 = 64 - __clzll(n0), bw3 = 64 - __clzll(n0 + 3);
-            if (n0 >= 3 && bw0 == bw3) {
-                const uint32_t thr = (uint32_t)(bw0 - 1) * 0x01010101u;
-                const uint32_t sieved = __vcmpgtu4(v & 0x7F7F7F7Fu, thr);  // every factor sieved
-                const uint32_t odd = __vcmpne4(v & 0x01010101u, 0u);
-                o = ((~(sieved ^ odd)) & 0xFEFEFEFEu) | 0x01010101u;       // -1 if odd == sieved_all
-                o &= __vcmpeq4(v & 0x80808080u, 0u);                        // square factor: 0
-            } else {
-                o = 0;
+        // 4. finalize to mu bytes in place, four at a time with byte-parallel
+        //    arithmetic.  With bits = bit_width(n), a byte a without the square
+        //    flag has every factor sieved iff a > bits - 1, i.e. iff bit 7 of
+        //    a + (0x7F - (bits - 1)) is set (no byte carries into the next); mu is
+        //    -1 where that bit equals a's parity bit, else 1.  A segment holds at
+        //    most one power of two above its start once low >= len (bits steps
+        //    there); the word straddling it, the words holding n <= 2 and the
+        //    first segments take the per-byte rule.  Bytes past len become 0.
+        {
+            const int bw_low = 64 - __clzll((u64)low);
+            const u64 pow2 = 1ull << bw_low;  // first n above low with a larger bit width
+            const uint32_t kbelow = (uint32_t)(0x7F - (bw_low - 1)) * 0x01010101u;
+            const uint32_t kabove = (uint32_t)(0x7F - bw_low) * 0x01010101u;
+            const bool simple = (u64)low >= 3 && (u64)low >= (u64)len;
+            const i64 edge = (i64)(pow2 - (u64)low);  // offset of pow2 in the segment
+            for (int i = tid; i < nw16; i += T) {
+                const uint32_t v = buf32[i];
+                const i64 j0 = 4 * (i64)i;
+                uint32_t o;
+                if (simple && (j0 + 3 < edge || j0 >= edge)) {
+                    const uint32_t t = (v & 0x7F7F7F7Fu) + (j0 < edge ? kbelow : kabove);
+                    const uint32_t x = ((t >> 7) ^ v) & 0x01010101u;         // 1: mu = +1, 0: mu = -1
+                    const uint32_t f = ((v >> 7) & 0x01010101u) * 0xFFu;   // square flag bytes
+                    o = ~f & (~(x * 0xFFu) | 0x01010101u);
+                } else {
+                    const u64 n0 = (u64)(low + j0);
+                    o = 0;
 #pragma unroll
-                for (int b = 0; b < 4; ++b) o |= finalize_byte((v >> (8 * b)) & 0xFFu, n0 + b) << (8 * b);
+                    for (int b = 0; b < 4; ++b) o |= finalize_byte((v >> (8 * b)) & 0xFFu, n0 + b) << (8 * b);
+                }
+                const int rem = len - 4 * i;
+                if (rem < 4) o = rem <= 0 ? 0u : (o & ((1u << (8 * rem)) - 1u));
+                buf32[i] = o;
             }
-            const int rem = len - 4 * i;
-            if (rem < 4) o = rem <= 0 ? 0u : (o & ((1u << (8 * rem)) - 1u));
-            buf32[i] = o;
         }
         __syncthreads();
 
@@ -313,6 +342,49 @@ void sieve_kernel_attrs(size_t smem, int block, int* per_sm) {
 
 void launch_sieve(const SieveArgs& a, int grid, int block, size_t smem, cudaStream_t s) {
     sieve_kernel<<<grid, block, smem, s>>>(a);
+}
+
+// segment of value n (1 <= n <= u_total) and its position there (dense segments
+// cover [seg*S + 1, ...], compressed ones [u_dense + (seg - dense_segs)*S + 1, ...])
+__device__ __forceinline__ void segment_of(u64 n, i64 u_dense, i64 dense_segs, int lgS, u64* seg, uint32_t* j) {
+    const u64 o = n <= (u64)u_dense ? n - 1 : n - 1 - (u64)u_dense;
+    const u64 k = o >> lgS;
+    *seg = n <= (u64)u_dense ? k : (u64)dense_segs + k;
+    *j = (uint32_t)(o - (k << lgS));
+}
+
+// one CTA per prime, threads over the multiples m*p^2
+__global__ void sq_bucket_count_kernel(const uint32_t* primes, int first, i64 u_total, i64 u_dense, i64 dense_segs,
+                                       int lgS, u64* counts) {
+    const u64 p = primes[first + blockIdx.x], sq = p * p;
+    for (u64 n = sq * (threadIdx.x + 1); n <= (u64)u_total; n += sq * blockDim.x) {
+        u64 seg;
+        uint32_t j;
+        segment_of(n, u_dense, dense_segs, lgS, &seg, &j);
+        atomicAdd(counts + seg, 1ull);
+    }
+}
+
+__global__ void sq_bucket_fill_kernel(const uint32_t* primes, int first, i64 u_total, i64 u_dense, i64 dense_segs,
+                                      int lgS, const u64* off, u64* cur, uint32_t* pos) {
+    const u64 p = primes[first + blockIdx.x], sq = p * p;
+    for (u64 n = sq * (threadIdx.x + 1); n <= (u64)u_total; n += sq * blockDim.x) {
+        u64 seg;
+        uint32_t j;
+        segment_of(n, u_dense, dense_segs, lgS, &seg, &j);
+        pos[off[seg] + atomicAdd(cur + seg, 1ull)] = j;
+    }
+}
+
+void launch_sq_bucket_count(const uint32_t* primes, int first, int n, i64 u_total, i64 u_dense, i64 dense_segs,
+                            int lgS, u64* counts, cudaStream_t s) {
+    if (n > first) sq_bucket_count_kernel<<<n - first, 128, 0, s>>>(primes, first, u_total, u_dense, dense_segs, lgS, counts);
+}
+
+void launch_sq_bucket_fill(const uint32_t* primes, int first, int n, i64 u_total, i64 u_dense, i64 dense_segs,
+                           int lgS, const u64* off, u64* cur, uint32_t* pos, cudaStream_t s) {
+    if (n > first)
+        sq_bucket_fill_kernel<<<n - first, 128, 0, s>>>(primes, first, u_total, u_dense, dense_segs, lgS, off, cur, pos);
 }
 
 // ---------------------------------------------------------------------------

@@ -25,6 +25,10 @@ struct SieveArgs {
     const uint32_t* primes;
     const u64* pinv;           // floor((2^64-1)/p) per prime: segment offsets without division
     const u64* sqinv;          // floor((2^64-1)/p^2) per prime
+    const double* prcp;        // RN(1/p) per prime (32-bit offset route; NULL: umod_inv only)
+    int sqC_first;             // first prime whose square is bucketed (p^2 > S); n_primes: none
+    const u64* sq_off;         // [nseg + 1]: bucketed square hits of each segment (NULL: no bucket)
+    const uint32_t* sq_pos;    // their positions within the segment
     const uint32_t* stencil4;  // 4 copies shifted by 0..3 bytes, kStencilWords each
     int16_t* dM;
     ulonglong2* planes;
@@ -77,6 +81,13 @@ struct SumsArgs {
 };
 
 void launch_sieve(const SieveArgs& a, int grid, int block, size_t smem, cudaStream_t s);
+// Bucketed squares: the multiples m*p^2 <= u_total of the primes p = primes[first..n)
+// (p^2 > S: at most one per segment), counted per segment, then written per segment
+// in the order of off = exclusive scan of the counts (cur: zeroed cursors).
+void launch_sq_bucket_count(const uint32_t* primes, int first, int n, i64 u_total, i64 u_dense, i64 dense_segs,
+                            int lgS, u64* counts, cudaStream_t s);
+void launch_sq_bucket_fill(const uint32_t* primes, int first, int n, i64 u_total, i64 u_dense, i64 dense_segs,
+                           int lgS, const u64* off, u64* cur, uint32_t* pos, cudaStream_t s);
 
 // Warp work items for the sieve's smaller moduli: the multiples of every prime
 // 13 <= p < S/32 (log weights) and of every square p^2 < S/32, p >= 5 (flags),

@@ -208,6 +208,10 @@ extern "C" int dr_table_build_noalloc(int device, void* stream, int64_t u_total,
         a.primes = d.scratch + kOffPrimes;
         a.pinv = (const u64*)(d.scratch + kOffPinv);
         a.sqinv = (const u64*)(d.scratch + kOffSqinv);
+        a.prcp = nullptr;  // offsets from the 64-bit reciprocals, squares without a bucket
+        a.sqC_first = a.n_primes;
+        a.sq_off = nullptr;
+        a.sq_pos = nullptr;
         a.stencil4 = d.scratch + kOffStencil;
         a.dM = dM;
         a.planes = (ulonglong2*)planes;
