@@ -134,7 +134,7 @@ inline void ref_compressed_params(int64_t X, dr_params* p) {
 // table is far cheaper to build on the GPU than on the CPU, so u is raised to
 // 0.6 (X / ln ln X)^(2/3) -- the reference's u formula without its 8e9 cap --
 // and cx = 1.3.  u is capped at 2.5e11 values (~80 GB of compressed tier) and
-// never below the endpoints.
+// never below the endpoints; the dense tier holds max(1.28e8, u/16) values (<= 4e9).
 inline void gpu_params(int64_t X, dr_params* p) {
     params_clear(p);
     const double cx = 1.3;
@@ -147,7 +147,10 @@ inline void gpu_params(int64_t X, dr_params* p) {
     int64_t endpoint = (int64_t)(cx * std::sqrt((double)X)) + 1000;
     u = std::max(u, std::max(S + 1000, endpoint));
     endpoint = (endpoint + 255) & ~255LL;
-    const int64_t u_dense = std::min(u, std::max(endpoint, std::min<int64_t>(128000000LL, ((u / 4 + 255) & ~255LL))));
+    // dense int16 tier: at least the reference's 1.28e8 and u/16 (at most 4e9): a larger
+    // tier lets the windowed S1 take more lookups (measured: ~1% at X = 10^16..10^18)
+    const int64_t dense_target = std::min<int64_t>(4000000000LL, std::max<int64_t>(128000000LL, u / 16));
+    const int64_t u_dense = std::min<int64_t>(u, std::max<int64_t>(endpoint, (dense_target + 255) & ~255LL));
     const int64_t N = X / u;
     const int64_t A_max = (int64_t)(cx * std::sqrt((double)X)) + 1000;
     p->u_total = u;
