@@ -231,6 +231,26 @@ __device__ __forceinline__ i64 candidate_k(i64 c) { return 3 * c + 1 + (c & 1); 
 
 enum { EVAL_NONE = 0, EVAL_SINGLE = 1, EVAL_COMB2 = 2 };
 
+// S1 segments: arithmetic progressions n = n0 + stride*i (stride 1, 2 or 6), or,
+// with stride code S1_WHEEL, the divisors coprime to 6 n = candidate_k(n0 + i)
+// (n0 then indexes the wheel).  Four segments per evaluation (kS1Seg).
+constexpr int kS1Seg = 4;
+enum { S1_WHEEL = 3 };
+
+__device__ __forceinline__ u64 s1_n_at(i64 n0, int st, u64 i) {
+    return st == S1_WHEEL ? (u64)candidate_k(n0 + (i64)i) : (u64)n0 + (u64)st * i;
+}
+
+// smallest wheel index c with candidate_k(c) >= n, largest with candidate_k(c) <= n (n >= 1)
+__device__ __forceinline__ i64 wheel_lower(i64 n) {
+    const i64 c = (n - 1) / 3;
+    return c + (candidate_k(c) < n ? 1 : 0);
+}
+__device__ __forceinline__ i64 wheel_upper(i64 n) {
+    const i64 c = (n - 1) / 3;
+    return c - (candidate_k(c) > n ? 1 : 0);
+}
+
 // Index ranges of one evaluation in op order: S1 segments first, then S2 pieces.
 struct EvalDesc {
     u64 y;
@@ -240,12 +260,12 @@ struct EvalDesc {
     int piece0;     // 9 (single) or 1 (comb2)
     int nseg;       // 2 + npieces
     i64 A, B, ky, ky2;
-    i64 s1_n0[2];
-    i64 s1_cnt[2];   // lookups of each S1 segment left to the sums kernel
-    i64 s1_full[2];  // all lookups of each S1 segment
-    u64 s1_wc[2];    // windows of each S1 segment summed by s1win_kernel
-    int s1_stride[2];
-    int s1_sign[2];
+    i64 s1_n0[kS1Seg];
+    i64 s1_cnt[kS1Seg];   // lookups of each S1 segment left to the sums kernel
+    i64 s1_full[kS1Seg];  // all lookups of each S1 segment
+    u64 s1_wc[kS1Seg];    // windows of each S1 segment summed by s1win_kernel
+    int s1_stride[kS1Seg];
+    int s1_sign[kS1Seg];
     i64 jlo[8], jhi[8];
     i64 mcnt[8];
     u64 total;
@@ -255,9 +275,35 @@ __device__ __forceinline__ i64 piece_mcount(i64 lo, i64 hi) {
     return lo > hi ? 0 : hi / 6 - lo / 6 + 1;
 }
 
+// The main S1 range of F(Y) (single) or of the odd-n sum of F(Y) - F(Y/2) (comb2):
+// n in [s, kap], s = floor(Y/u) + 1 (rounded up to odd for comb2), kap = kappa_Y.
+__device__ __forceinline__ void s1_main(const QueryDev& Q, u64 Y, bool comb2, i64* s, i64* kap) {
+    const i64 A = split_point(Q.cx, (i64)Y);
+    *kap = (i64)udiv(Y, (u64)(A + 1));
+    i64 st = (i64)udiv(Y, (u64)Q.u) + 1;
+    if (comb2 && (st & 1) == 0) ++st;
+    *s = st;
+}
+
+__device__ __forceinline__ void s1_set(EvalDesc& d, int g, i64 n0, int stride, i64 last, int sign) {
+    d.s1_n0[g] = n0;
+    d.s1_stride[g] = stride;
+    d.s1_sign[g] = sign;
+    if (stride == S1_WHEEL) d.s1_cnt[g] = last >= 0 && last >= n0 ? last - n0 + 1 : 0;  // n0, last: wheel indices
+    else d.s1_cnt[g] = last >= n0 ? (last - n0) / stride + 1 : 0;
+}
+
 // Decode evaluation e (0/1) of candidate c of query Q.  Follows the outer
 // reduction of mertens_dr.hpp:1470-1485, 1616-1632 and the ranges of
 // eval_single_S (:1490-1525) and eval_comb2 (:1527-1614).
+//
+// S1 terms that cancel between the two evaluations of a candidate are left out:
+// for k <= N/3 the second evaluation works on y/3 with the opposite sign, and its
+// term M(floor(floor(y/3)/n')) = M(floor(y/(3n'))) at odd n' equals the first
+// evaluation's term at n = 3n'.  Wherever both exist -- odd n' in [clo, chi] with
+// 3*clo >= s0, 3*chi <= kappa_y -- both are dropped: the first evaluation keeps its
+// odd n coprime to 3 (the wheel) and the multiples of 3 outside [3clo, 3chi], the
+// second its divisors outside [clo, chi].  The S1 total is unchanged term for term.
 __device__ inline void decode_eval(const QueryDev& Q, const TableView& T, i64 c, int e, EvalDesc& d) {
     d.kind = EVAL_NONE;
     d.total = 0;
@@ -285,15 +331,33 @@ __device__ inline void decode_eval(const QueryDev& Q, const TableView& T, i64 c,
         else return;
     }
     d.y = y;
-    const u64 u = (u64)Q.u;
+    for (int g = 0; g < kS1Seg; ++g) s1_set(d, g, 0, 2, -1, 1);
+    // cancelled odd n' in [clo, chi] of y/3 (ranges 1, 2)
+    i64 s0 = 0, kap0 = 0, s1 = 0, kap1 = 0, clo = 1, chi = -1;
+    if (range <= 2) {
+        s1_main(Q, yk, true, &s0, &kap0);
+        s1_main(Q, yk / 3, range == 1, &s1, &kap1);
+        i64 lo = max(s1, (s0 + 2) / 3);
+        if ((lo & 1) == 0) ++lo;
+        i64 hi = min(kap1, kap0 / 3);
+        if ((hi & 1) == 0) --hi;
+        clo = lo;
+        chi = hi;
+    }
+    const bool cancel = clo <= chi;
     if (d.kind == EVAL_SINGLE) {
         const i64 A = split_point(Q.cx, (i64)y);
         const i64 ky = (i64)udiv(y, (u64)(A + 1));
-        const i64 start = (i64)udiv(y, u) + 1;
+        const i64 start = (i64)udiv(y, (u64)Q.u) + 1;
         d.A = A; d.B = 0; d.ky = ky; d.ky2 = 0;
-        d.s1_n0[0] = start; d.s1_stride[0] = 1; d.s1_sign[0] = 1;
-        d.s1_cnt[0] = ky >= start ? ky - start + 1 : 0;
-        d.s1_n0[1] = 0; d.s1_stride[1] = 2; d.s1_sign[1] = 1; d.s1_cnt[1] = 0;
+        if (e == 1 && cancel) {  // range 2: all n' of [start, ky] but the odd ones in [clo, chi]
+            const i64 so = start | 1;
+            s1_set(d, 0, so, 2, clo - 2, 1);
+            s1_set(d, 1, chi + 2, 2, ky, 1);
+            s1_set(d, 2, (start + 1) & ~1ll, 2, ky, 1);
+        } else {
+            s1_set(d, 0, start, 1, ky, 1);
+        }
         d.npieces = 4; d.piece0 = 9;
         const i64 a6 = A / 6, a3 = A / 3, a2 = A / 2;
         d.jlo[0] = 1;      d.jhi[0] = a6;
@@ -306,19 +370,28 @@ __device__ inline void decode_eval(const QueryDev& Q, const TableView& T, i64 c,
         const i64 ky = (i64)udiv(y, (u64)(A + 1));
         const i64 ky2 = (i64)udiv(y2, (u64)(B + 1));
         const i64 two = 2 * ky2;
-        i64 start = (i64)udiv(y, u) + 1;
+        i64 start = (i64)udiv(y, (u64)Q.u) + 1;
         if ((start & 1) == 0) ++start;
         d.A = A; d.B = B; d.ky = ky; d.ky2 = ky2;
-        d.s1_n0[0] = start; d.s1_stride[0] = 2; d.s1_sign[0] = 1;
-        d.s1_cnt[0] = ky >= start ? (ky - start) / 2 + 1 : 0;
+        if (e == 0 && cancel) {  // odd n of [start, ky]: the wheel + multiples of 3 outside [3clo, 3chi]
+            s1_set(d, 0, wheel_lower(start), S1_WHEEL, wheel_upper(ky), 1);
+            i64 m3 = start;  // first odd multiple of 3 >= start
+            while (m3 % 3) m3 += 2;
+            s1_set(d, 1, m3, 6, 3 * clo - 6, 1);
+            s1_set(d, 2, 3 * chi + 6, 6, ky, 1);
+        } else if (e == 1 && cancel) {  // range 1: odd n' of [start, ky] outside [clo, chi]
+            s1_set(d, 0, start, 2, clo - 2, 1);
+            s1_set(d, 1, chi + 2, 2, ky, 1);
+        } else {
+            s1_set(d, 0, start, 2, ky, 1);
+        }
         // even-n correction between kappa_y and 2*kappa_{y/2} (:1568-1610)
         i64 e0 = 0, last = -1;
         int sg = 1;
         if (two > ky) { e0 = ky + 1; last = two; sg = -1; }
         else if (two < ky) { e0 = two + 1; last = ky; sg = 1; }
         if (e0 & 1) ++e0;
-        d.s1_n0[1] = e0; d.s1_stride[1] = 2; d.s1_sign[1] = sg;
-        d.s1_cnt[1] = last >= e0 ? (last - e0) / 2 + 1 : 0;
+        s1_set(d, 3, e0, 2, last, sg);
         d.npieces = 8; d.piece0 = 1;
         const i64 b6 = B / 6, a6 = A / 6, b3 = B / 3, a3 = A / 3, b2 = B / 2, a2 = A / 2;
         d.jlo[0] = 1;      d.jhi[0] = b6;
@@ -330,23 +403,26 @@ __device__ inline void decode_eval(const QueryDev& Q, const TableView& T, i64 c,
         d.jlo[6] = a2 + 1; d.jhi[6] = B;
         d.jlo[7] = B + 1;  d.jhi[7] = A;
     }
-    d.nseg = 2 + d.npieces;
+    d.nseg = kS1Seg + d.npieces;
     // windowed S1: the lookups with q < wc*W, i.e. n > y/(wc*W), go to s1win_kernel
-    for (int g = 0; g < 2; ++g) {
+    for (int g = 0; g < kS1Seg; ++g) {
         d.s1_full[g] = d.s1_cnt[g];
         d.s1_wc[g] = 0;
         const i64 cnt = d.s1_cnt[g];
         if (cnt <= 0 || Q.win == 0) continue;
-        const i64 nlast = d.s1_n0[g] + (i64)d.s1_stride[g] * (cnt - 1);
+        const int st = d.s1_stride[g];
+        const i64 nlast = (i64)s1_n_at(d.s1_n0[g], st, (u64)(cnt - 1));
         // the windowed kernel divides on the 32-bit route with tabulated reciprocals
         if (nlast >= (1ll << 31) || (u64)nlast > Q.inv_limit) continue;
-        const u64 wc = s1_win_count(y, d.s1_stride[g], Q.win, Q.win_max);
+        const u64 wc = s1_win_count(y, st, Q.win, Q.win_max);  // the wheel's density is that of stride 3
         if (wc == 0) continue;
         const i64 ncut = (i64)udiv(y, wc * Q.win) + 1;  // n >= ncut <=> q < wc*W
         d.s1_wc[g] = wc;
-        d.s1_cnt[g] = ncut <= d.s1_n0[g] ? 0 : min(cnt, (ncut - 1 - d.s1_n0[g]) / d.s1_stride[g] + 1);
+        if (st == S1_WHEEL) d.s1_cnt[g] = min(cnt, max(0ll, wheel_upper(ncut - 1) - d.s1_n0[g] + 1));
+        else d.s1_cnt[g] = ncut <= d.s1_n0[g] ? 0 : min(cnt, (ncut - 1 - d.s1_n0[g]) / st + 1);
     }
-    u64 tot = (u64)d.s1_cnt[0] + (u64)d.s1_cnt[1];
+    u64 tot = 0;
+    for (int g = 0; g < kS1Seg; ++g) tot += (u64)d.s1_cnt[g];
     for (int p = 0; p < d.npieces; ++p) {
         d.mcnt[p] = piece_mcount(d.jlo[p], d.jhi[p]);
         tot += (u64)d.mcnt[p];

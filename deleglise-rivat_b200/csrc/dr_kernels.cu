@@ -468,12 +468,12 @@ __global__ void plan_kernel(const QueryDev* __restrict__ qs, int nq, const Table
         if (wdesc && Q.win) {
             S1WinDesc w;
             w.y = d.y;
-            for (int g = 0; g < 2; ++g) {
+            for (int g = 0; g < kS1Seg; ++g) {
                 const bool on = d.kind != EVAL_NONE && d.s1_full[g] > 0 && d.s1_wc[g] > 0;
                 w.n0[g] = on ? (uint32_t)d.s1_n0[g] : 0u;
                 w.cnt[g] = on ? (uint32_t)d.s1_full[g] : 0u;
                 w.wc[g] = on ? (uint32_t)d.s1_wc[g] : 0u;
-                w.w0[g] = on ? (uint32_t)(udiv(d.y, (u64)(d.s1_n0[g] + (i64)d.s1_stride[g] * (d.s1_full[g] - 1))) /
+                w.w0[g] = on ? (uint32_t)(udiv(d.y, s1_n_at(d.s1_n0[g], d.s1_stride[g], (u64)(d.s1_full[g] - 1))) /
                                           Q.win)
                              : 0u;
                 w.sg[g] = on ? (int32_t)(d.coef * d.s1_sign[g]) * d.s1_stride[g] : 0;
@@ -486,8 +486,12 @@ __global__ void plan_kernel(const QueryDev* __restrict__ qs, int nq, const Table
             unsigned long long* cq = reinterpret_cast<unsigned long long*>(counts + 4 * qi);
             if ((local & 1) == 0) atomicAdd(cq + 0, 1ull);
             atomicAdd(cq + 1, 1ull);
-            const u64 s1d = (u64)d.s1_cnt[0] + (u64)d.s1_cnt[1];  // left to the sums kernel
-            atomicAdd(cq + 2, (u64)d.s1_full[0] + (u64)d.s1_full[1]);
+            u64 s1d = 0, s1f = 0;  // lookups left to the sums kernel, all lookups
+            for (int g = 0; g < kS1Seg; ++g) {
+                s1d += (u64)d.s1_cnt[g];
+                s1f += (u64)d.s1_full[g];
+            }
+            atomicAdd(cq + 2, s1f);
             atomicAdd(cq + 3, d.total - s1d);
         }
     }
@@ -627,17 +631,17 @@ __device__ __forceinline__ double u32_to_double(uint32_t v) {
 }
 
 // 1/n for the kS1Unroll divisors n = nfirst + nstep*k of a lane's group
-// (nfirst + nstep*(kS1Unroll-1) < 2^31).  From nfirst >= 2^14 on, only 1/nfirst
+// (nfirst + nstep*(kS1Unroll-1) < 2^31).  From nfirst >= 256*nstep on, only 1/nfirst
 // is loaded; the others start from the first-order Taylor value r0*(1 -
-// k*nstep*r0), relative error (k*nstep/nfirst)^2 <= 2^-10.4, and two Newton steps
+// k*nstep*r0), relative error (k*nstep/nfirst)^2 <= (7/256)^2 = 2^-10.4, and two Newton steps
 // r += r*(1 - n*r) square that error twice (to below 2^-41, on the FP64 pipe,
 // which the loop leaves idle) -- far inside what the 32-bit dense route needs
-// (q <= u_dense < 2^31).  Below 2^14 every reciprocal is loaded.  This cuts the
+// (q <= u_dense < 2^31).  Below that every reciprocal is loaded.  This cuts the
 // L2 traffic of the reciprocal table by a factor kS1Unroll where the loop is
 // bound by it.
 __device__ __forceinline__ void rcp_group(const double* rcp, uint32_t nfirst, uint32_t nstep, double nstep_d,
                                           double* rv) {
-    if (nfirst >= (1u << 14)) {
+    if (nfirst >= 256u * nstep) {
         const double r0 = __ldg(rcp + nfirst);
         const double xr = nstep_d * r0 * r0;
         const double nd = u32_to_double(nfirst);
@@ -668,7 +672,9 @@ __device__ __forceinline__ i64 s1_part(const SumsArgs& a, u64 y, i64 n0, int str
     i64 acc = 0;
     const u64 lim = (u64)a.inv_limit;
     const u64 lim31 = min(lim, (u64)0x7FFFFFFF);
-    const uint32_t nstep = 32u * (uint32_t)stride;
+    // a lane's divisors form an arithmetic progression: i -> i + 32 adds 32*stride,
+    // or 96 on the wheel (candidate_k keeps its parity pattern every 32 steps)
+    const uint32_t nstep = stride == S1_WHEEL ? 96u : 32u * (uint32_t)stride;
     const double nstep_d = u32_to_double(nstep);
     const double yd = __ull2double_rn(y);
     const uint32_t ylo = (uint32_t)y;
@@ -679,7 +685,8 @@ __device__ __forceinline__ i64 s1_part(const SumsArgs& a, u64 y, i64 n0, int str
     const u64 span = 32ull * (kS1Unroll - 1);
     const uint32_t groups = il + span < i1 ? (uint32_t)((i1 - il - span - 1) / (32ull * kS1Unroll) + 1) : 0u;
     const u64 gstep = (u64)nstep * kS1Unroll;
-    u64 nfirst = (u64)n0 + (u64)stride * il;
+    const u64 nl = s1_n_at(n0, stride, il);  // this lane's first divisor
+    u64 nfirst = nl;
     for (uint32_t g = 0; g < groups; ++g, nfirst += gstep) {
         const u64 nlast = nfirst + (u64)nstep * (kS1Unroll - 1);
         if (nlast <= lim31) {
@@ -711,10 +718,9 @@ __device__ __forceinline__ i64 s1_part(const SumsArgs& a, u64 y, i64 n0, int str
             }
         }
     }
-    for (u64 i = il + 32ull * kS1Unroll * groups; i < i1; i += 32) {
-        const u64 n = (u64)n0 + (u64)stride * i;
+    u64 n = nl + gstep * groups;
+    for (u64 i = il + 32ull * kS1Unroll * groups; i < i1; i += 32, n += nstep)
         acc += table_M(a.T, n <= lim ? udiv_rcp(y, yd, (uint32_t)n, __ldg(a.rcp + n)) : udiv(y, n));
-    }
     return acc;
 }
 
@@ -955,17 +961,17 @@ __global__ void __launch_bounds__(256, DRB_SUMS_MINB) sums_kernel(const SumsArgs
             const int nseg = d.nseg;
             u64 segstart = 0;
             for (int g = 0; g < nseg && segstart < hi; ++g) {
-                const u64 cnt = g < 2 ? (u64)d.s1_cnt[g] : (u64)d.mcnt[g - 2];
+                const u64 cnt = g < kS1Seg ? (u64)d.s1_cnt[g] : (u64)d.mcnt[g - kS1Seg];
                 const u64 sb = segstart;
                 segstart += cnt;
                 const u64 a0 = max(lo, sb), a1 = min(hi, segstart);
                 if (a0 >= a1) continue;
-                if (g < 2) {
+                if (g < kS1Seg) {
                     const i64 part = s1_part(a, y, d.s1_n0[g], d.s1_stride[g], a0 - sb, a1 - sb, lane);
                     const i64 sg = coef * d.s1_sign[g];
                     s1 += sg > 0 ? (u64)part : (u64)(-part);
                 } else {
-                    const int p = g - 2;
+                    const int p = g - kS1Seg;
                     const u64 part = s2_dispatch(a, sT, y, d.piece0 + p, d.jlo[p], d.jhi[p], (u64)d.mcnt[p], a0 - sb,
                                                  a1 - sb, lane);
                     s2 += coef > 0 ? part : (u64)(0 - part);
@@ -998,27 +1004,28 @@ __global__ void __launch_bounds__(256, DRB_SUMS_MINB) sums_kernel(const SumsArgs
 // ---------------------------------------------------------------------------
 constexpr int kWinThreads = 512;
 
-// sum of M(q) over n = na + st*i, i < cnt, q in the window [qbase, qbase + W) (qbase a
-// multiple of W, so q - qbase = q & (W - 1)); lanes take consecutive n.  The
-// reciprocal loads mostly hit L1 (neighbouring windows reuse the same divisors).
+// sum of M(q) over a segment's divisors in the window [qbase, qbase + W) (qbase a
+// multiple of W, so q - qbase = q & (W - 1)): lanes take consecutive divisors, so a
+// lane's divisors are nl, nl + nstep, ... (nstep = 32*stride, 96 on the wheel), cntl
+// of them.  The reciprocal loads mostly hit L1 (neighbouring windows reuse them).
 __device__ __forceinline__ int32_t s1win_range(const int16_t* win, uint32_t wmask, const double* rcp, double yd,
-                                               uint32_t ylo, uint32_t na, uint32_t st, uint32_t cnt, int lane) {
+                                               uint32_t ylo, uint32_t nl, uint32_t nstep, uint32_t cntl) {
     int32_t part = 0;
     const int16_t* w7 = win + 7;
-    uint32_t i = (uint32_t)lane;
-    for (; i + 96u < cnt; i += 128u) {
+    uint32_t t = 0;
+    for (; t + 3 < cntl; t += 4) {
         uint32_t n[4];
         double r[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            n[k] = na + st * (i + 32u * k);
+            n[k] = nl + nstep * (t + k);
             r[k] = __ldg(rcp + n[k]);
         }
 #pragma unroll
         for (int k = 0; k < 4; ++k) part += w7[qfix(qest(yd, r[k]), ylo, n[k]) & wmask];
     }
-    for (; i < cnt; i += 32u) {
-        const uint32_t nn = na + st * i;
+    for (; t < cntl; ++t) {
+        const uint32_t nn = nl + nstep * t;
         part += w7[qfix(qest(yd, __ldg(rcp + nn)), ylo, nn) & wmask];
     }
     return part;
@@ -1069,26 +1076,38 @@ __global__ void __launch_bounds__(kWinThreads, 2) s1win_kernel(const S1WinArgs a
 #pragma unroll 1
             for (int e = 0; e < 2; ++e) {
                 const S1WinDesc D = a.desc[Q.slot_base + 2ull * c + (u64)e];
-                const bool on0 = D.cnt[0] && D.w0[0] <= I.w && I.w < D.wc[0];
-                const bool on1 = D.cnt[1] && D.w0[1] <= I.w && I.w < D.wc[1];
-                if (!(on0 || on1)) continue;
+                bool any = false;
+#pragma unroll
+                for (int g = 0; g < kS1Seg; ++g) any |= D.cnt[g] && D.w0[g] <= I.w && I.w < D.wc[g];
+                if (!any) continue;
                 const double yd = __ull2double_rn(D.y);
-                // n in (y/qhi, y/qlo]  <=>  floor(y/n) in [qlo, qhi)
+                // n in (y/qhi, y/qlo]  <=>  floor(y/n) in [qlo, qhi);
                 // exact quotients: udiv_rcp while y/q < 2^50 (q < 2^31 here), else udiv
                 const u64 nlo = ((D.y >> 50) < qhi ? udiv_rcp(D.y, yd, (uint32_t)qhi, rhi) : udiv(D.y, qhi)) + 1;
                 const u64 nhi = qlo == 0 ? ~0ull
                                          : (D.y >> 50) < qlo ? udiv_rcp(D.y, yd, (uint32_t)qlo, rlo) : udiv(D.y, qlo);
 #pragma unroll 1
-                for (int g = 0; g < 2; ++g) {
-                    if (!(g == 0 ? on0 : on1)) continue;
-                    const uint32_t st = (uint32_t)(D.sg[g] < 0 ? -D.sg[g] : D.sg[g]);
-                    const u64 n0 = D.n0[g], nend = n0 + (u64)st * (D.cnt[g] - 1);
-                    u64 na = max(n0, nlo);
-                    if (st == 2) na += (na - n0) & 1;  // strides are 1 or 2
-                    const u64 nb = min(nend, nhi);
-                    if (na > nb) continue;
-                    const uint32_t cnt = (uint32_t)((nb - na) / st + 1);
-                    const int32_t part = s1win_range(win, wmask, a.rcp, yd, (uint32_t)D.y, (uint32_t)na, st, cnt, lane);
+                for (int g = 0; g < kS1Seg; ++g) {
+                    if (!(D.cnt[g] && D.w0[g] <= I.w && I.w < D.wc[g])) continue;
+                    const int st = D.sg[g] < 0 ? -D.sg[g] : D.sg[g];
+                    // index range [ia, ib] of the segment's divisors in [nlo, nhi]
+                    i64 ia, ib;
+                    if (st == S1_WHEEL) {
+                        ia = max((i64)0, wheel_lower((i64)nlo) - (i64)D.n0[g]);
+                        ib = min((i64)D.cnt[g] - 1, nhi > 0x7FFFFFFFull ? (i64)D.cnt[g] - 1
+                                                                     : wheel_upper((i64)nhi) - (i64)D.n0[g]);
+                    } else {
+                        ia = nlo <= D.n0[g] ? 0 : (i64)((nlo - D.n0[g] + st - 1) / st);
+                        ib = nhi < D.n0[g] ? -1
+                             : nhi > 0x7FFFFFFFull ? (i64)D.cnt[g] - 1  // window 0: no upper bound
+                                                   : min((i64)D.cnt[g] - 1, (i64)((nhi - D.n0[g]) / st));
+                    }
+                    if (ia > ib) continue;
+                    const u64 cnt = (u64)(ib - ia + 1);
+                    const uint32_t cntl = cnt > (u64)lane ? (uint32_t)((cnt - lane + 31) >> 5) : 0u;
+                    const uint32_t nstep = st == S1_WHEEL ? 96u : 32u * (uint32_t)st;
+                    const uint32_t nl = (uint32_t)s1_n_at(D.n0[g], st, (u64)(ia + lane));
+                    const int32_t part = s1win_range(win, wmask, a.rcp, yd, (uint32_t)D.y, nl, nstep, cntl);
                     acc += D.sg[g] > 0 ? (i64)part : -(i64)part;
                 }
             }

@@ -37,16 +37,16 @@ struct SieveArgs {
     int32_t* seg_sum;
 };
 
-// One evaluation as seen by s1win_kernel (written by plan_kernel): its two S1
-// segments n = n0 + |sg|*i, i < cnt, with sign sg/|sg| (mu(k) times the segment's
-// sign), and the windows [w0, wc) in which each segment has windowed lookups.
+// One evaluation as seen by s1win_kernel (written by plan_kernel): its S1 segments
+// (divisors s1_n_at(n0, |sg|, i), i < cnt) with sign sg/|sg| (mu(k) times the
+// segment's sign), and the windows [w0, wc) in which each segment has windowed lookups.
 struct S1WinDesc {
     u64 y;
-    uint32_t n0[2];
-    uint32_t cnt[2];
-    uint32_t w0[2];  // first window holding a lookup: floor(y / n_last) / W
-    uint32_t wc[2];
-    int32_t sg[2];   // +-stride; 0: no S1 segment
+    uint32_t n0[kS1Seg];   // first divisor (first wheel index for S1_WHEEL segments)
+    uint32_t cnt[kS1Seg];
+    uint32_t w0[kS1Seg];   // first window holding a lookup: floor(y / n_last) / W
+    uint32_t wc[kS1Seg];
+    int32_t sg[kS1Seg];    // +-stride code (1, 2, 6 or S1_WHEEL); 0: no S1 segment
 };
 
 // Work item of s1win_kernel: window w of query q, evaluation candidates [c0, c1).

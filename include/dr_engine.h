@@ -63,8 +63,7 @@ typedef struct {
     int32_t block_threads;/* threads per sieve CTA (0: default)                 */
     int32_t chunk_log2;  /* S1/S2 work item = 2^chunk_log2 ops (0: default)    */
     int32_t s1_window_log2; /* windowed S1 of a single query: windows of 2^k
-                               table values, k in 12..16 (0: 15 from X = 3e15
-                               on, off below; negative: off) */
+                               table values, k in 12..16 (0 or negative: off) */
 } dr_params;
 
 typedef struct {

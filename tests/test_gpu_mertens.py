@@ -115,7 +115,7 @@ def test_windowed_s1_matches_direct(engine):
     all.  Both give the same M(X), the same C/S1/S2 checksums and the same S1 op
     count, for every window length and for inputs that reach window 0."""
     cases = [(10**9 + 7, 12), (2 * 10**10 + 1, 13), (10**11, 14), (3 * 10**12, 15), (10**14, 16), (10**15, 15),
-             (10**16, 0)]
+             (10**16, 15)]
     for X, wl in cases:
         p = dr_b200.default_params(X, dr_b200.POLICY_GPU)
         on = dr_b200.Params(**{**p.as_dict(), "s1_window_log2": wl})
