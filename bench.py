@@ -347,17 +347,17 @@ def run_engine(args, world, rank, local):
     peak, peak_kind = load_peaks()
     s0_ = stats[0]
     phases = {"table_ms": tab, "plan_ms": plan, "sums_ms": sums}
-    # dominant phase: S1/S2 (s1win_kernel + sums_kernel), timed together by the
-    # engine's CUDA events.  Algorithmic bytes: the Mertens value of every S1
+    # dominant phase: S1/S2 (sums_kernel; with the windowed S1 switched on, s1win_kernel
+    # as well), timed by the engine's CUDA events.  Algorithmic bytes: the Mertens value of every S1
     # lookup (2 B, int16 dense tier) and the Mobius bits of every S2 wheel position
     # (0.5 B); reciprocal tables are a cache of this implementation and are not
     # counted.  ops_per_s is the figure the kernels are optimised on.
     alg = 2 * s0_.s1_ops + 0.5 * s0_.s2_ops
     achieved = alg / (sums / 1e3) / 1e9
-    # DRAM traffic: ncu dram__bytes_read.sum + dram__bytes_write.sum of both S1/S2
-    # kernels in a 1-pass capture of M(10^16) (profiles/s1win_kernel_m4e15.md):
-    # 96.8 GB for 6.15e10 ops = 1.58 B per op, times this call's op count.
-    traffic = 1.58 * (s0_.s1_ops + s0_.s2_ops)
+    # DRAM traffic: ncu dram__bytes_read.sum + dram__bytes_write.sum of sums_kernel
+    # in a 1-pass capture of M(10^16) with these parameters (profiles/launches_m1e16.md):
+    # 91.9 GB for 5.33e10 ops = 1.72 B per op, times this call's op count.
+    traffic = 1.72 * (s0_.s1_ops + s0_.s2_ops)
     line = {
         "metric": "sec per M(10^16)" if X == X_HEADLINE else f"sec per M({X})", "value": value, "unit": "s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_per * 1e3,
@@ -374,11 +374,11 @@ def run_engine(args, world, rank, local):
         "gpu_launches": launches,
         "e2e": {"value": host_per / world, "unit": "s", "h2d_bytes_per_step": int(s0_.h2d_bytes),
                 "d2h_bytes_per_step": int(s0_.d2h_bytes)},
-        "roofline": {"bound": "hbm", "kernel": "s1win_kernel + sums_kernel (S1/S2 phase)", "achieved": achieved,
+        "roofline": {"bound": "hbm", "kernel": "sums_kernel (S1/S2 phase)", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                     "traffic_basis": "ncu DRAM bytes per op of both S1/S2 kernels at M(10^16), times the op count",
+                     "traffic_basis": "ncu DRAM bytes per op of sums_kernel at M(10^16), times the op count",
                      "ops": {"s1_lookups": s0_.s1_ops, "s2_positions": s0_.s2_ops},
-                     "note": "the windowed S1 is bound by the L1/shared pipe (86%), the sums kernel by random DRAM sectors of its far S1 lookups (2.35 TB/s); ops_per_s = S1 lookups + S2 positions per second",
+                     "note": "sums_kernel: far S1 lookups cost a random DRAM sector each (1.3 TB/s of 32 B sectors), near ones and the S2 wheel stream hit L2; issue 57% active; ops_per_s = S1 lookups + S2 positions per second",
                      "ops_per_s": (s0_.s1_ops + s0_.s2_ops) / (sums / 1e3)},
         "clocks": clocks.summary(),
         "batched": batch,
