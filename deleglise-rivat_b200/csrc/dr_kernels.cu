@@ -123,11 +123,13 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
 
         // 1. periodic stencil: weights of 2,3,5,7,11 and flags of 4, 9 (:818-823)
         {
-            const uint32_t ph0 = (uint32_t)(base % kStencilPeriod);
+            // stencil phase of word i: (base + 4i) mod the period, stepped by 4T
+            uint32_t ph = (uint32_t)((base + 4 * (i64)tid) % kStencilPeriod);
+            const uint32_t step = (4u * (uint32_t)T) % (uint32_t)kStencilPeriod;
             for (int i = tid; i < nw16; i += T) {
-                uint32_t ph = ph0 + 4u * (uint32_t)i;
-                ph %= (uint32_t)kStencilPeriod;
                 buf32[i] = __ldg(a.stencil4 + (ph & 3u) * kStencilWords + (ph >> 2));
+                ph += step;
+                if (ph >= (uint32_t)kStencilPeriod) ph -= (uint32_t)kStencilPeriod;
             }
         }
         __syncthreads();
@@ -264,21 +266,49 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
                 }
             }
         } else {
-            // 64-value words: nonzero / negative planes by ballot, local checkpoint
+            // 64-value words, one per thread: nonzero / negative planes and the local
+            // checkpoint.  A mu byte is 0, 1 or 0xFF, so its bit 0 is the nonzero bit
+            // and its bit 7 the negative bit; per 4-byte shared word both are moved
+            // to bits 0 and 4 of each byte and gathered into two nibbles (bits 24..27:
+            // nonzero, 28..31: negative) by one multiply, whose partial products land
+            // on distinct bits.  Lane l reads its 16 words starting at word l/2, which
+            // puts the 32 lanes of a warp on 32 distinct banks; the planes are rotated
+            // back by 4*(l/2) bits at the end.  Words past nw16 read as 0.
             const i64 wbase = (base - a.u_dense) >> 6;
             const int nwords = (len + 63) >> 6;
-            for (int w = warp; w < nwords; w += nwarps) {
-                const int i0 = 64 * w + lane, i1 = i0 + 32;
-                const int v0 = i0 < len ? (int)(int8_t)buf[i0] : 0;
-                const int v1 = i1 < len ? (int)(int8_t)buf[i1] : 0;
-                const uint32_t nz0 = __ballot_sync(0xffffffffu, v0 != 0);
-                const uint32_t nz1 = __ballot_sync(0xffffffffu, v1 != 0);
-                const uint32_t ng0 = __ballot_sync(0xffffffffu, v0 < 0);
-                const uint32_t ng1 = __ballot_sync(0xffffffffu, v1 < 0);
-                if (lane == 0) {
-                    a.planes[wbase + w] = make_ulonglong2((u64)nz0 | ((u64)nz1 << 32), (u64)ng0 | ((u64)ng1 << 32));
-                    a.ckpt[wbase + w] = gs[4 * w];
+            const uint32_t rot = (uint32_t)(lane >> 1);
+            for (int w = tid; w < nwords; w += T) {
+                const uint32_t* src = buf32 + 16 * w;
+                const bool full = 16 * w + 16 <= nw16;
+                uint32_t zl = 0, zh = 0, gl = 0, gh = 0;
+#pragma unroll
+                for (int k = 0; k < 16; ++k) {
+                    const uint32_t kk = ((uint32_t)k + rot) & 15u;
+                    const uint32_t v = (full || 16 * w + (int)kk < nw16) ? src[kk] : 0u;
+                    const uint32_t x = (v & 0x01010101u) | ((v >> 3) & 0x10101010u);
+                    const uint32_t pr = x * 0x01020408u;
+                    const uint32_t z = (pr >> 24) & 0xFu, g = pr >> 28;
+                    if (k < 8) {
+                        zl |= z << (4 * k);
+                        gl |= g << (4 * k);
+                    } else {
+                        zh |= z << (4 * (k - 8));
+                        gh |= g << (4 * (k - 8));
+                    }
                 }
+                if (rot >= 8u) {
+                    uint32_t t = zl;
+                    zl = zh;
+                    zh = t;
+                    t = gl;
+                    gl = gh;
+                    gh = t;
+                }
+                const uint32_t sh = (4u * rot) & 31u;
+                const u64 nz = ((u64)__funnelshift_l(zl, zh, sh) << 32) | __funnelshift_l(zh, zl, sh);
+                const u64 neg = ((u64)__funnelshift_l(gl, gh, sh) << 32) | __funnelshift_l(gh, gl, sh);
+                a.planes[wbase + w] = make_ulonglong2(nz, neg);
+                a.ckpt[wbase + w] = gs[4 * w];
             }
         }
         // Mobius wheel bits for j <= mu_limit coprime to 6; groups of 32 m
