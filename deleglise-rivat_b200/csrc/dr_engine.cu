@@ -69,6 +69,7 @@ struct dr_ctx {
     uint64_t held = 0;
     // table buffers
     DevBuf dM, planes, ckpt, wheel, seg_sum, seg_off, primes, pinv, items, stencil, prcp;
+    DevBuf items_odd, stencil_odd, dplanes;  // odd-mode sieve: items, stencil, dense-tier plane words
     DevBuf sq_cnt, sq_off, sq_cur, sq_pos, sq_tmp;  // bucketed square hits per segment
     // query buffers
     DevBuf queries, ops, prefix, scan_tmp, acc, counts, ticket, misc, inv, invw, wdesc, witems;
@@ -224,32 +225,6 @@ const std::vector<uint32_t>& primes_upto(dr_ctx* c, int64_t root) {
     return c->host_primes;
 }
 
-// 4 copies of the periodic stencil shifted by 0..3 bytes (entry i describes
-// n = i + 1: weights of 2,3,5,7,11 and square flags of 4 and 9).
-std::vector<uint32_t> make_stencil4() {
-    std::vector<uint8_t> st(kStencilPeriod + 8);
-    const unsigned small[5] = {2, 3, 5, 7, 11};
-    for (int i = 0; i < kStencilPeriod + 8; ++i) {
-        const int n = (i % kStencilPeriod) + 1;
-        unsigned a = 0;
-        for (unsigned p : small)
-            if (n % (int)p == 0) a += (unsigned)((32 - __builtin_clz(p - 1)) | 1);
-        if (n % 4 == 0 || n % 9 == 0) a |= 0x80u;
-        st[(size_t)i] = (uint8_t)a;
-    }
-    std::vector<uint32_t> out((size_t)4 * kStencilWords);
-    for (int s = 0; s < 4; ++s)
-        for (int w = 0; w < kStencilWords; ++w) {
-            uint32_t v = 0;
-            for (int b = 0; b < 4; ++b) {
-                const size_t idx = (size_t)(4 * w + s + b);
-                v |= (uint32_t)(idx < st.size() ? st[idx] : 0) << (8 * b);
-            }
-            out[(size_t)s * kStencilWords + (size_t)w] = v;
-        }
-    return out;
-}
-
 int64_t num_candidates(int64_t N) {  // k <= N with gcd(k, 6) = 1
     if (N <= 0) return 0;
     const int64_t r = N % 6;
@@ -344,22 +319,27 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     };
     a.sq_first = first_at_least(5);
     a.w_first = first_at_least(13);
-    a.tierB_first = std::max(a.w_first, first_at_least((uint32_t)std::max(13, S / 32)));
-    {
-        // first prime whose square reaches S/32
-        int k = a.sq_first;
-        while (k < (int)pr.size() && (uint64_t)pr[k] * pr[k] < (uint64_t)(S / 32)) ++k;
-        a.sqB_first = k;
-    }
-    std::vector<uint4> items(kMaxSieveItems);
-    a.n_items = build_sieve_items(pr.data(), (int)pr.size(), S, items.data(), kMaxSieveItems);
-    if ((rc = ensure(c, c->items, (size_t)std::max(a.n_items, 1) * 16))) return rc;
-    if (a.n_items) {
-        const void* si = stage_put(c, items.data(), (size_t)a.n_items * 16);
-        if (!si) return fail(DR_ERR_NOMEM, "internal: staging area too small");
-        CU(cudaMemcpyAsync(c->items.p, si, (size_t)a.n_items * 16, cudaMemcpyHostToDevice, c->stream));
-    }
-    a.items = (const uint4*)c->items.p;
+    // B sieved bytes per segment (S in full mode, S/2 in odd mode): warp items for the
+    // moduli below B/32, one thread per prime above
+    auto set_moduli = [&](SieveArgs& m, int B, DevBuf& buf) -> int {
+        m.tierB_first = std::max(m.w_first, first_at_least((uint32_t)std::max(13, B / 32)));
+        int k = m.sq_first;  // first prime whose square reaches B/32
+        while (k < (int)pr.size() && (uint64_t)pr[k] * pr[k] < (uint64_t)(B / 32)) ++k;
+        m.sqB_first = k;
+        std::vector<uint4> items(kMaxSieveItems);
+        m.n_items = build_sieve_items(pr.data(), (int)pr.size(), B, items.data(), kMaxSieveItems);
+        int e = ensure(c, buf, (size_t)std::max(m.n_items, 1) * 16);
+        if (e) return e;
+        if (m.n_items) {
+            const void* si = stage_put(c, items.data(), (size_t)m.n_items * 16);
+            if (!si) return fail(DR_ERR_NOMEM, "internal: staging area too small");
+            if (cudaMemcpyAsync(buf.p, si, (size_t)m.n_items * 16, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+                return fail(DR_ERR_CUDA, "sieve items upload failed");
+        }
+        m.items = (const uint4*)buf.p;
+        return DR_OK;
+    };
+    if ((rc = set_moduli(a, S, c->items))) return rc;
     a.primes = (const uint32_t*)c->primes.p;
     a.pinv = (const u64*)c->pinv.p;
     a.sqinv = (const u64*)c->pinv.p + pr.size();
@@ -384,17 +364,31 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
         a.sq_pos = (const uint32_t*)c->sq_pos.p;
     }
     a.stencil4 = (const uint32_t*)c->stencil.p;
+    a.stencil_odd4 = (const uint32_t*)c->stencil_odd.p;
     a.dM = (int16_t*)c->dM.p;
     a.planes = (ulonglong2*)c->planes.p;
     a.ckpt = (int32_t*)c->ckpt.p;
     a.wheel = (uint4*)c->wheel.p;
     a.seg_sum = (int32_t*)c->seg_sum.p;
+    a.dplanes = nullptr;
 
-    const size_t smem = sieve_smem_bytes(S);
-    int per_sm = 0;
-    sieve_kernel_attrs(smem, block, &per_sm);
-    if (per_sm < 1) per_sm = 1;
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(nseg, (int64_t)c->sm_count * per_sm));
+    // Launch plan: the first wave of segments in full mode, the rest in odd mode,
+    // in launches [b0, b1) whose halves lie below b0 (ranges roughly doubling).
+    const size_t smem_f = sieve_smem_bytes(S, false), smem_o = sieve_smem_bytes(S, true);
+    int per_f = 0, per_o = 0;
+    sieve_kernel_attrs(smem_f, false, block, &per_f);
+    sieve_kernel_attrs(smem_o, true, block, &per_o);
+    const int64_t grid_f = (int64_t)c->sm_count * std::max(per_f, 1);
+    const int64_t grid_o = (int64_t)c->sm_count * std::max(per_o, 1);
+    const int64_t first_odd = std::min<int64_t>(nseg, grid_f);
+    const bool odd = sieve_odd_ok(u_dense, nseg, first_odd);
+    SieveArgs ao = a;
+    if (odd) {
+        if ((rc = ensure(c, c->dplanes, (size_t)(u_dense / 64 + 1) * 16))) return rc;
+        a.dplanes = (ulonglong2*)c->dplanes.p;
+        ao = a;
+        if ((rc = set_moduli(ao, S / 2, c->items_odd))) return rc;
+    }
 
     CU(record_event(c, 0));
     CU(cudaMemsetAsync(c->wheel.p, 0, (size_t)wheel_groups * 16, c->stream));
@@ -411,8 +405,23 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
         CU(cudaGetLastError());
         launches += 5;
     }
-    launch_sieve(a, grid, block, smem, c->stream);
+    a.seg_begin = 0;
+    a.seg_end = odd ? first_odd : nseg;
+    launch_sieve(a, false, (int)std::max<int64_t>(1, std::min<int64_t>(a.seg_end, grid_f)), block, smem_f, c->stream);
     CU(cudaGetLastError());
+    for (int64_t b0 = a.seg_end; b0 < nseg;) {
+        int64_t b1 = sieve_odd_range_end(b0, nseg, dense_segs, u_dense, u_total, S);
+        const bool use_odd = b1 > b0;
+        if (!use_odd) b1 = nseg;  // never expected: the rest in full mode
+        SieveArgs& m = use_odd ? ao : a;
+        m.seg_begin = b0;
+        m.seg_end = b1;
+        launch_sieve(m, use_odd, (int)std::min<int64_t>(b1 - b0, use_odd ? grid_o : grid_f), block,
+                     use_odd ? smem_o : smem_f, c->stream);
+        CU(cudaGetLastError());
+        ++launches;
+        b0 = b1;
+    }
     launch_seg_scan((const int32_t*)c->seg_sum.p, (int32_t*)c->seg_off.p, nseg, c->stream);
     CU(cudaGetLastError());
     launch_fixup((int16_t*)c->dM.p, u_dense, S, (const int32_t*)c->seg_off.p, (int32_t*)c->ckpt.p, nwords,
@@ -839,12 +848,15 @@ int dr_ctx_create(int device, void* cuda_stream, dr_ctx** out) {
     for (auto& e : c->ev) cudaEventCreate(&e);
     init_piece_constants();
     std::vector<uint32_t> st = make_stencil4();
+    std::vector<uint32_t> sto = make_stencil_odd4();
     int rc = ensure(c, c->stencil, st.size() * 4);
+    if (!rc) rc = ensure(c, c->stencil_odd, sto.size() * 4);
     if (rc) {
         dr_ctx_destroy(c);
         return rc;
     }
     cudaMemcpy(c->stencil.p, st.data(), st.size() * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(c->stencil_odd.p, sto.data(), sto.size() * 4, cudaMemcpyHostToDevice);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         dr_ctx_destroy(c);
@@ -861,7 +873,7 @@ int dr_ctx_destroy(dr_ctx* c) {
     DevBuf* bufs[] = {&c->dM, &c->planes, &c->ckpt, &c->wheel, &c->seg_sum, &c->seg_off, &c->primes, &c->pinv, &c->items, &c->stencil,
                       &c->queries, &c->ops, &c->prefix, &c->scan_tmp, &c->acc, &c->counts, &c->ticket, &c->misc,
                       &c->inv, &c->invw, &c->wdesc, &c->witems, &c->prcp, &c->sq_cnt, &c->sq_off, &c->sq_cur,
-                      &c->sq_pos, &c->sq_tmp};
+                      &c->sq_pos, &c->sq_tmp, &c->items_odd, &c->stencil_odd, &c->dplanes};
     for (DevBuf* b : bufs) release(c, *b);
     drop_graphs(c);
     if (c->pinned) cudaFreeHost(c->pinned);
@@ -916,8 +928,9 @@ uint64_t dr_table_bytes(int64_t u_total, int64_t u_dense, int64_t mu_limit) {
     const int64_t nseg = (u_total + 4095) / 4096 + 2;
     // + bucketed square hits: u * sum over primes p^2 > S of 1/p^2 < u / (sqrt(S) ln sqrt(S)),
     // 4 bytes each, for the default S = 2^17 (at most 0.0019 u bytes)
-    return (uint64_t)u_dense * 2 + (uint64_t)nwords * 20 + (uint64_t)(mu_limit / 192 + 2) * 16 + (uint64_t)nseg * 32 +
-           (uint64_t)u_total / 500;
+    // + the dense tier's plane words (16 bytes per 64 values) that the odd-mode sieve reads
+    return (uint64_t)u_dense * 2 + (uint64_t)(u_dense / 64 + 1) * 16 + (uint64_t)nwords * 20 +
+           (uint64_t)(mu_limit / 192 + 2) * 16 + (uint64_t)nseg * 32 + (uint64_t)u_total / 500;
 }
 
 uint64_t dr_query_bytes(int64_t X, const dr_params* p) {

@@ -98,38 +98,154 @@ __device__ __forceinline__ uint32_t finalize_byte(uint32_t acc, u64 n) {
     return (odd == sieved_all) ? 0xFFu : 1u;
 }
 
-size_t sieve_smem_bytes(int S) { return (size_t)S + (size_t)(S / 16) * 4 + 64; }
+// Shared memory of a sieve CTA.  Full mode: the S-byte segment and 16-value group
+// sums.  Odd mode: S/2 bytes (the odd values), 64-value word sums and plane words.
+size_t sieve_smem_bytes(int S, bool odd) {
+    return odd ? (size_t)S / 2 + (size_t)(S / 64) * 4 + (size_t)(S / 64) * 16 + 64
+               : (size_t)S + (size_t)(S / 16) * 4 + 64;
+}
+
+// {nonzero, negative} plane words of 64 consecutive mu bytes src[16w .. 16w+16)
+// (words at or past nw16 read as 0), one 64-value word per thread.  A mu byte is 0,
+// 1 or 0xFF, so bit 0 is its nonzero bit and bit 7 its negative bit; per shared word
+// both are moved to bits 0 and 4 of each byte and gathered into two nibbles (bits
+// 24..27: nonzero, 28..31: negative) by one multiply, whose partial products land on
+// distinct bits.  Lane l reads its 16 words starting at word l/2, which puts the 32
+// lanes of a warp on 32 distinct banks; the planes are rotated back by 4*(l/2) bits.
+__device__ __forceinline__ void planes_of_bytes(const uint32_t* buf32, int w, int nw16, int lane, u64* nz,
+                                                u64* neg) {
+    const uint32_t rot = (uint32_t)(lane >> 1);
+    const uint32_t* src = buf32 + 16 * w;
+    const bool full = 16 * w + 16 <= nw16;
+    uint32_t zl = 0, zh = 0, gl = 0, gh = 0;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        const uint32_t kk = ((uint32_t)k + rot) & 15u;
+        const uint32_t v = (full || 16 * w + (int)kk < nw16) ? src[kk] : 0u;
+        const uint32_t x = (v & 0x01010101u) | ((v >> 3) & 0x10101010u);
+        const uint32_t pr = x * 0x01020408u;
+        const uint32_t z = (pr >> 24) & 0xFu, g = pr >> 28;
+        if (k < 8) {
+            zl |= z << (4 * k);
+            gl |= g << (4 * k);
+        } else {
+            zh |= z << (4 * (k - 8));
+            gh |= g << (4 * (k - 8));
+        }
+    }
+    if (rot >= 8u) {
+        uint32_t t = zl;
+        zl = zh;
+        zh = t;
+        t = gl;
+        gl = gh;
+        gh = t;
+    }
+    const uint32_t sh = (4u * rot) & 31u;
+    *nz = ((u64)__funnelshift_l(zl, zh, sh) << 32) | __funnelshift_l(zh, zl, sh);
+    *neg = ((u64)__funnelshift_l(gl, gh, sh) << 32) | __funnelshift_l(gh, gl, sh);
+}
+
+// bit k of x -> bit 2k of the result (k < 32)
+__device__ __forceinline__ uint32_t spread16(uint32_t x) {
+    x = (x | (x << 8)) & 0x00FF00FFu;
+    x = (x | (x << 4)) & 0x0F0F0F0Fu;
+    x = (x | (x << 2)) & 0x33333333u;
+    return (x | (x << 1)) & 0x55555555u;
+}
+__device__ __forceinline__ u64 spread32(uint32_t x) {
+    return ((u64)spread16(x >> 16) << 32) | spread16(x & 0xFFFFu);
+}
+
+// Plane words of 64-value word w of an odd-mode segment (values base+1+64w+b, b <
+// 64).  Odd values (even b) from the mu bytes buf8[32w + b/2], i.e. the 8 shared
+// words 8w.., lane l starting at word (l/4) & 7 (conflict-free for a warp of
+// consecutive w): per word the nonzero and negative bits of its 4 bytes land on bits
+// 0, 2, 4, 6 of a byte by one multiply each (partial products on distinct bits).
+// Even values 2m (odd b = 2k+1, m = base/2 + 32w + k + 1) from the plane bits of m:
+// mu(2m) = -mu(m) for odd m (k even), 0 for even m; the 32 values m are one aligned
+// half of a plane word (base/2 + 32w is a multiple of 32).
+__device__ __forceinline__ void planes_odd_mode(const SieveArgs& a, const uint32_t* buf32, int w, int nw16,
+                                                int lane, i64 base, u64* nz, u64* neg) {
+    const uint32_t rot = (uint32_t)(lane >> 2) & 7u;
+    const uint32_t* src = buf32 + 8 * w;
+    const bool full = 8 * w + 8 <= nw16;
+    uint32_t zl = 0, zh = 0, gl = 0, gh = 0;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const uint32_t tt = ((uint32_t)t + rot) & 7u;
+        const uint32_t v = (full || 8 * w + (int)tt < nw16) ? src[tt] : 0u;
+        const uint32_t z = ((v & 0x01010101u) * 0x01041040u) >> 24;         // bits 0, 2, 4, 6
+        const uint32_t g = (((v >> 7) & 0x01010101u) * 0x01041040u) >> 24;
+        if (t < 4) {
+            zl |= z << (8 * t);
+            gl |= g << (8 * t);
+        } else {
+            zh |= z << (8 * (t - 4));
+            gh |= g << (8 * (t - 4));
+        }
+    }
+    if (rot >= 4u) {
+        uint32_t t = zl;
+        zl = zh;
+        zh = t;
+        t = gl;
+        gl = gh;
+        gh = t;
+    }
+    const uint32_t sh = (8u * rot) & 31u;
+    u64 z = ((u64)__funnelshift_l(zl, zh, sh) << 32) | __funnelshift_l(zh, zl, sh);
+    u64 g = ((u64)__funnelshift_l(gl, gh, sh) << 32) | __funnelshift_l(gh, gl, sh);
+    const i64 q0 = (base >> 1) + 32 * (i64)w;  // 0-based bit index of m = q0 + 1
+    const i64 G = q0 >> 6;
+    const ulonglong2 P = G < (a.u_dense >> 6) ? __ldg(a.dplanes + G) : __ldg(a.planes + (G - (a.u_dense >> 6)));
+    const uint32_t hz = (uint32_t)(((q0 >> 5) & 1) ? P.x >> 32 : P.x);
+    const uint32_t hg = (uint32_t)(((q0 >> 5) & 1) ? P.y >> 32 : P.y);
+    z |= spread32(hz & 0x55555555u) << 1;
+    g |= spread32(hz & ~hg & 0x55555555u) << 1;
+    *nz = z;
+    *neg = g;
+}
 
 // ---------------------------------------------------------------------------
-// Segmented byte-log Mobius sieve + table outputs.
+// Segmented byte-log Mobius sieve + table outputs (ODD: odd values only).
 // ---------------------------------------------------------------------------
+template <bool ODD>
 __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint8_t* buf = smem;
     uint32_t* buf32 = reinterpret_cast<uint32_t*>(smem);
-    int32_t* gs = reinterpret_cast<int32_t*>(smem + a.S);
+    int32_t* gs = reinterpret_cast<int32_t*>(smem + (ODD ? a.S / 2 : a.S));
+    ulonglong2* wpl = reinterpret_cast<ulonglong2*>(smem + a.S / 2 + (a.S / 64) * 4);  // ODD only
     __shared__ int32_t wtot[33];
 
     const int T = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = T >> 5;
 
-    for (i64 seg = blockIdx.x; seg < a.nseg; seg += gridDim.x) {
+    for (i64 seg = a.seg_begin + blockIdx.x; seg < a.seg_end; seg += gridDim.x) {
         const bool dense = seg < a.dense_segs;
         const i64 base = dense ? seg * (i64)a.S : a.u_dense + (seg - a.dense_segs) * (i64)a.S;
         const i64 end = min(base + (i64)a.S, dense ? a.u_dense : a.u_total);
         const int len = (int)(end - base);
         const i64 low = base + 1;
-        const int ng = (len + 15) >> 4;  // 16-value groups
-        const int nw16 = ng * 4;         // words covering the groups
+        // sieved bytes: value low + j (full) or the odd value low + 2j (ODD; low is odd)
+        const int nb = ODD ? (len + 1) >> 1 : len;
+        const int ng = (nb + 15) >> 4;  // 16-byte groups
+        const int nw16 = ng * 4;        // words covering the groups
 
-        // 1. periodic stencil: weights of 2,3,5,7,11 and flags of 4, 9 (:818-823)
+        // 1. periodic stencil: weights of 2,3,5,7,11 and flags of 4, 9 (:818-823);
+        //    ODD: weights of 3,5,7,11 and the flag of 9 on the odd values.  The
+        //    phase of word i, (p0 + 4i) mod the period, is stepped by 4T.
         {
-            // stencil phase of word i: (base + 4i) mod the period, stepped by 4T
-            uint32_t ph = (uint32_t)((base + 4 * (i64)tid) % kStencilPeriod);
-            const uint32_t step = (4u * (uint32_t)T) % (uint32_t)kStencilPeriod;
+            const uint32_t P = ODD ? (uint32_t)kStencilOddPeriod : (uint32_t)kStencilPeriod;
+            const uint32_t* st = ODD ? a.stencil_odd4 : a.stencil4;
+            const uint32_t W = ODD ? (uint32_t)kStencilOddWords : (uint32_t)kStencilWords;
+            const i64 p0 = ODD ? base >> 1 : base;
+            uint32_t ph = (uint32_t)((p0 + 4 * (i64)tid) % P);
+            const uint32_t step = (4u * (uint32_t)T) % P;
             for (int i = tid; i < nw16; i += T) {
-                buf32[i] = __ldg(a.stencil4 + (ph & 3u) * kStencilWords + (ph >> 2));
+                buf32[i] = __ldg(st + (ph & 3u) * W + (ph >> 2));
                 ph += step;
-                if (ph >= (uint32_t)kStencilPeriod) ph -= (uint32_t)kStencilPeriod;
+                if (ph >= P) ph -= P;
             }
         }
         __syncthreads();
@@ -137,18 +253,22 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
         // 2-3. square flags for p >= 5 (:824-829) and log weights for p >= 13
         //    (:830-835).  Flags are idempotent ORs; weight bytes stay below 0x80,
         //    so a 32-bit add of w << 8*(j&3) never carries into a neighbour and
-        //    the order of the marks does not matter.
+        //    the order of the marks does not matter.  ODD: the odd multiples only,
+        //    consecutive ones 2m apart in value, m apart in bytes.
         //    Smaller moduli: balanced warp items (lanes stride the multiples).
         for (int it = warp; it < a.n_items; it += nwarps) {
             const uint4 I = __ldg(a.items + it);
-            if (I.y >= (uint32_t)len) continue;
+            if (I.y >= (uint32_t)nb) continue;
             const uint32_t m = I.x;
             const bool sq = (I.w >> 31) != 0;
             const uint32_t pidx = I.w & 0x7fffffffu;
             const u64 inv = sq ? __ldg(a.sqinv + pidx) : __ldg(a.pinv + pidx);
-            const uint32_t r = (uint32_t)umod_inv((u64)low + I.y, m, inv);
-            uint32_t j = I.y + (r ? m - r : 0u) + (uint32_t)lane * m;
-            const uint32_t jend = min((uint32_t)len, I.y + 1024u * m);
+            const u64 v0 = (u64)low + (ODD ? 2ull * I.y : (u64)I.y);  // value of byte I.y
+            const uint32_t r = (uint32_t)umod_inv(v0, m, inv);
+            uint32_t d = r ? m - r : 0u;  // first multiple: v0 + d
+            if (ODD && (d & 1u)) d += m;  // v0 is odd: the first odd multiple
+            uint32_t j = I.y + (ODD ? d >> 1 : d) + (uint32_t)lane * m;
+            const uint32_t jend = min((uint32_t)nb, I.y + 1024u * m);
             if (sq) {
                 for (; j < jend; j += 32u * m) atomicOr(&buf32[j >> 2], 0x80u << ((j & 3) * 8));
             } else {
@@ -158,20 +278,26 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
         }
         //    Larger moduli (at most 32 hits per segment): one prime per thread.
         //    Squares above S hit a segment at most once: their hits come from
-        //    the per-segment bucket (sq_off / sq_pos) when there is one.
+        //    the per-segment bucket (sq_off / sq_pos: value offsets) when there is one.
         const int sq_end = a.sq_off ? a.sqC_first : a.n_primes;
         for (int i = a.sqB_first + tid; i < sq_end; i += T) {
             const u64 p = a.primes[i];
             const u64 sq = p * p;
             if (sq > (u64)end) break;
             const u64 r = umod_inv((u64)low, sq, a.sqinv[i]);
-            for (u64 j = r ? sq - r : 0; j < (u64)len; j += sq)
+            u64 d = r ? sq - r : 0;
+            if (ODD && (d & 1)) d += sq;
+            for (u64 j = ODD ? d >> 1 : d; j < (u64)nb; j += sq)
                 atomicOr(&buf32[j >> 2], 0x80u << ((j & 3) * 8));
         }
         if (a.sq_off) {
             const u64 h1 = __ldg(a.sq_off + seg + 1);
             for (u64 h = __ldg(a.sq_off + seg) + tid; h < h1; h += T) {
-                const uint32_t j = __ldg(a.sq_pos + h);
+                uint32_t j = __ldg(a.sq_pos + h);
+                if (ODD) {
+                    if (j & 1u) continue;  // even value
+                    j >>= 1;
+                }
                 atomicOr(&buf32[j >> 2], 0x80u << ((j & 3) * 8));
             }
         }
@@ -186,7 +312,9 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
                 r = (uint32_t)low - qfix(qest(lowd, __ldg(a.prcp + i)), (uint32_t)low, p) * p;
             else
                 r = (uint32_t)umod_inv((u64)low, p, a.pinv[i]);
-            for (uint32_t j = r ? p - r : 0; j < (uint32_t)len; j += p)
+            uint32_t d = r ? p - r : 0;
+            if (ODD && (d & 1u)) d += p;
+            for (uint32_t j = ODD ? d >> 1 : d; j < (uint32_t)nb; j += p)
                 atomicAdd(&buf32[j >> 2], w << ((j & 3) * 8));
         }
         __syncthreads();
@@ -198,14 +326,15 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
         //    -1 where that bit equals a's parity bit, else 1.  A segment holds at
         //    most one power of two above its start once low >= len (bits steps
         //    there); the word straddling it, the words holding n <= 2 and the
-        //    first segments take the per-byte rule.  Bytes past len become 0.
+        //    first segments take the per-byte rule.  Bytes past nb become 0.
         {
             const int bw_low = 64 - __clzll((u64)low);
             const u64 pow2 = 1ull << bw_low;  // first n above low with a larger bit width
             const uint32_t kbelow = (uint32_t)(0x7F - (bw_low - 1)) * 0x01010101u;
             const uint32_t kabove = (uint32_t)(0x7F - bw_low) * 0x01010101u;
             const bool simple = (u64)low >= 3 && (u64)low >= (u64)len;
-            const i64 edge = (i64)(pow2 - (u64)low);  // offset of pow2 in the segment
+            // first byte whose value reaches pow2
+            const i64 edge = ODD ? (i64)((pow2 - (u64)low + 1) >> 1) : (i64)(pow2 - (u64)low);
             for (int i = tid; i < nw16; i += T) {
                 const uint32_t v = buf32[i];
                 const i64 j0 = 4 * (i64)i;
@@ -216,101 +345,19 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
                     const uint32_t f = ((v >> 7) & 0x01010101u) * 0xFFu;   // square flag bytes
                     o = ~f & (~(x * 0xFFu) | 0x01010101u);
                 } else {
-                    const u64 n0 = (u64)(low + j0);
+                    const u64 n0 = (u64)(low + (ODD ? 2 * j0 : j0));
                     o = 0;
 #pragma unroll
-                    for (int b = 0; b < 4; ++b) o |= finalize_byte((v >> (8 * b)) & 0xFFu, n0 + b) << (8 * b);
+                    for (int b = 0; b < 4; ++b)
+                        o |= finalize_byte((v >> (8 * b)) & 0xFFu, n0 + (ODD ? 2 * b : b)) << (8 * b);
                 }
-                const int rem = len - 4 * i;
+                const int rem = nb - 4 * i;
                 if (rem < 4) o = rem <= 0 ? 0u : (o & ((1u << (8 * rem)) - 1u));
                 buf32[i] = o;
             }
         }
         __syncthreads();
 
-        // 5. 16-value group sums and their exclusive scan
-        for (int g = tid; g < ng; g += T) {
-            const uint4 v = reinterpret_cast<const uint4*>(buf)[g];
-            int s = __dp4a((int)v.x, 0x01010101, 0);
-            s = __dp4a((int)v.y, 0x01010101, s);
-            s = __dp4a((int)v.z, 0x01010101, s);
-            s = __dp4a((int)v.w, 0x01010101, s);
-            gs[g] = s;
-        }
-        __syncthreads();
-        const int total = block_excl_scan(gs, ng, wtot);
-
-        // 6. outputs
-        if (dense) {
-            // dM[i] = M(i+1) local to the segment; offsets added by fixup_kernel
-            int16_t* out = a.dM + base;
-            for (int g = tid; g < ng; g += T) {
-                const uint4 v = reinterpret_cast<const uint4*>(buf)[g];
-                int run = gs[g];
-                uint32_t pk[8];
-                const uint32_t words[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-                for (int b = 0; b < 16; b += 2) {
-                    run += (int)(int8_t)((words[b >> 2] >> (8 * (b & 3))) & 0xFFu);
-                    const uint32_t lo = (uint32_t)(run & 0xFFFF);
-                    run += (int)(int8_t)((words[(b + 1) >> 2] >> (8 * ((b + 1) & 3))) & 0xFFu);
-                    pk[b >> 1] = lo | ((uint32_t)(run & 0xFFFF) << 16);
-                }
-                if (16 * g + 16 <= len) {
-                    uint4* dst = reinterpret_cast<uint4*>(out + 16 * g);
-                    dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-                    dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
-                } else {
-                    for (int b = 0; b < len - 16 * g; ++b)
-                        out[16 * g + b] = (int16_t)((pk[b >> 1] >> (16 * (b & 1))) & 0xFFFFu);
-                }
-            }
-        } else {
-            // 64-value words, one per thread: nonzero / negative planes and the local
-            // checkpoint.  A mu byte is 0, 1 or 0xFF, so its bit 0 is the nonzero bit
-            // and its bit 7 the negative bit; per 4-byte shared word both are moved
-            // to bits 0 and 4 of each byte and gathered into two nibbles (bits 24..27:
-            // nonzero, 28..31: negative) by one multiply, whose partial products land
-            // on distinct bits.  Lane l reads its 16 words starting at word l/2, which
-            // puts the 32 lanes of a warp on 32 distinct banks; the planes are rotated
-            // back by 4*(l/2) bits at the end.  Words past nw16 read as 0.
-            const i64 wbase = (base - a.u_dense) >> 6;
-            const int nwords = (len + 63) >> 6;
-            const uint32_t rot = (uint32_t)(lane >> 1);
-            for (int w = tid; w < nwords; w += T) {
-                const uint32_t* src = buf32 + 16 * w;
-                const bool full = 16 * w + 16 <= nw16;
-                uint32_t zl = 0, zh = 0, gl = 0, gh = 0;
-#pragma unroll
-                for (int k = 0; k < 16; ++k) {
-                    const uint32_t kk = ((uint32_t)k + rot) & 15u;
-                    const uint32_t v = (full || 16 * w + (int)kk < nw16) ? src[kk] : 0u;
-                    const uint32_t x = (v & 0x01010101u) | ((v >> 3) & 0x10101010u);
-                    const uint32_t pr = x * 0x01020408u;
-                    const uint32_t z = (pr >> 24) & 0xFu, g = pr >> 28;
-                    if (k < 8) {
-                        zl |= z << (4 * k);
-                        gl |= g << (4 * k);
-                    } else {
-                        zh |= z << (4 * (k - 8));
-                        gh |= g << (4 * (k - 8));
-                    }
-                }
-                if (rot >= 8u) {
-                    uint32_t t = zl;
-                    zl = zh;
-                    zh = t;
-                    t = gl;
-                    gl = gh;
-                    gh = t;
-                }
-                const uint32_t sh = (4u * rot) & 31u;
-                const u64 nz = ((u64)__funnelshift_l(zl, zh, sh) << 32) | __funnelshift_l(zh, zl, sh);
-                const u64 neg = ((u64)__funnelshift_l(gl, gh, sh) << 32) | __funnelshift_l(gh, gl, sh);
-                a.planes[wbase + w] = make_ulonglong2(nz, neg);
-                a.ckpt[wbase + w] = gs[4 * w];
-            }
-        }
         // Mobius wheel bits for j <= mu_limit coprime to 6; groups of 32 m
         // may straddle segments, hence atomicOr into the zeroed wheel.
         if (low <= a.mu_limit) {
@@ -319,8 +366,8 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
             for (i64 g = g0 + warp; g <= g1; g += nwarps) {
                 const i64 m = 32 * g + lane;
                 const i64 j1 = 6 * m + 1, j5 = 6 * m + 5;
-                const int v1 = (j1 >= low && j1 <= hi) ? (int)(int8_t)buf[j1 - low] : 0;
-                const int v5 = (j5 >= low && j5 <= hi) ? (int)(int8_t)buf[j5 - low] : 0;
+                const int v1 = (j1 >= low && j1 <= hi) ? (int)(int8_t)buf[ODD ? (j1 - low) >> 1 : j1 - low] : 0;
+                const int v5 = (j5 >= low && j5 <= hi) ? (int)(int8_t)buf[ODD ? (j5 - low) >> 1 : j5 - low] : 0;
                 const uint32_t a1 = __ballot_sync(0xffffffffu, v1 != 0);
                 const uint32_t b1 = __ballot_sync(0xffffffffu, v1 < 0);
                 const uint32_t a5 = __ballot_sync(0xffffffffu, v5 != 0);
@@ -331,6 +378,113 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
                     if (b1) atomicOr(wp + 1, b1);
                     if (a5) atomicOr(wp + 2, a5);
                     if (b5) atomicOr(wp + 3, b5);
+                }
+            }
+        }
+
+        const int nwords = (len + 63) >> 6;  // 64-value words
+        int total;
+        if (ODD) {
+            // 5. plane words of the segment (odd values sieved, even ones from their
+            //    halves), their Mobius sums and exclusive scan
+            const u64 lastmask = (len & 63) ? (1ull << (len & 63)) - 1 : ~0ull;
+            for (int w = tid; w < nwords; w += T) {
+                u64 nz, neg;
+                planes_odd_mode(a, buf32, w, nw16, lane, base, &nz, &neg);
+                if (w == nwords - 1) {
+                    nz &= lastmask;
+                    neg &= lastmask;
+                }
+                gs[w] = __popcll(nz) - 2 * __popcll(neg);
+                wpl[w] = make_ulonglong2(nz, neg);
+                if (dense) a.dplanes[(base >> 6) + w] = make_ulonglong2(nz, neg);
+                else a.planes[((base - a.u_dense) >> 6) + w] = make_ulonglong2(nz, neg);
+            }
+            __syncthreads();
+            total = block_excl_scan(gs, nwords, wtot);
+            if (dense) {
+                // 6. dM[i] = M(i+1) local to the segment, 16 values per thread
+                int16_t* out = a.dM + base;
+                for (int g = tid; g < 4 * nwords; g += T) {
+                    const int w = g >> 2, sub = g & 3;
+                    const ulonglong2 P = wpl[w];
+                    const u64 below = sub ? (1ull << (16 * sub)) - 1 : 0ull;
+                    int run = gs[w] + __popcll(P.x & below) - 2 * __popcll(P.y & below);
+                    const uint32_t z = (uint32_t)(P.x >> (16 * sub)) & 0xFFFFu;
+                    const uint32_t n = (uint32_t)(P.y >> (16 * sub)) & 0xFFFFu;
+                    uint32_t pk[8];
+#pragma unroll
+                    for (int b = 0; b < 16; b += 2) {
+                        run += (int)((z >> b) & 1u) - 2 * (int)((n >> b) & 1u);
+                        const uint32_t lo = (uint32_t)(run & 0xFFFF);
+                        run += (int)((z >> (b + 1)) & 1u) - 2 * (int)((n >> (b + 1)) & 1u);
+                        pk[b >> 1] = lo | ((uint32_t)(run & 0xFFFF) << 16);
+                    }
+                    if (16 * g + 16 <= len) {
+                        uint4* dst = reinterpret_cast<uint4*>(out + 16 * g);
+                        dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                        dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+                    } else {
+                        for (int b = 0; b < len - 16 * g; ++b)
+                            out[16 * g + b] = (int16_t)((pk[b >> 1] >> (16 * (b & 1))) & 0xFFFFu);
+                    }
+                }
+            } else {
+                int32_t* ck = a.ckpt + ((base - a.u_dense) >> 6);
+                for (int w = tid; w < nwords; w += T) ck[w] = gs[w];
+            }
+        } else {
+            // 5. 16-value group sums and their exclusive scan
+            for (int g = tid; g < ng; g += T) {
+                const uint4 v = reinterpret_cast<const uint4*>(buf)[g];
+                int s = __dp4a((int)v.x, 0x01010101, 0);
+                s = __dp4a((int)v.y, 0x01010101, s);
+                s = __dp4a((int)v.z, 0x01010101, s);
+                s = __dp4a((int)v.w, 0x01010101, s);
+                gs[g] = s;
+            }
+            __syncthreads();
+            total = block_excl_scan(gs, ng, wtot);
+
+            // 6. outputs
+            if (dense) {
+                // dM[i] = M(i+1) local to the segment; offsets added by fixup_kernel
+                int16_t* out = a.dM + base;
+                for (int g = tid; g < ng; g += T) {
+                    const uint4 v = reinterpret_cast<const uint4*>(buf)[g];
+                    int run = gs[g];
+                    uint32_t pk[8];
+                    const uint32_t words[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                    for (int b = 0; b < 16; b += 2) {
+                        run += (int)(int8_t)((words[b >> 2] >> (8 * (b & 3))) & 0xFFu);
+                        const uint32_t lo = (uint32_t)(run & 0xFFFF);
+                        run += (int)(int8_t)((words[(b + 1) >> 2] >> (8 * ((b + 1) & 3))) & 0xFFu);
+                        pk[b >> 1] = lo | ((uint32_t)(run & 0xFFFF) << 16);
+                    }
+                    if (16 * g + 16 <= len) {
+                        uint4* dst = reinterpret_cast<uint4*>(out + 16 * g);
+                        dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                        dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+                    } else {
+                        for (int b = 0; b < len - 16 * g; ++b)
+                            out[16 * g + b] = (int16_t)((pk[b >> 1] >> (16 * (b & 1))) & 0xFFFFu);
+                    }
+                }
+            }
+            if (!dense || a.dplanes) {
+                // 64-value plane words (compressed tier, or the dense scratch planes
+                // that odd-mode segments read) and the local checkpoints
+                for (int w = tid; w < nwords; w += T) {
+                    u64 nz, neg;
+                    planes_of_bytes(buf32, w, nw16, lane, &nz, &neg);
+                    if (dense) {
+                        a.dplanes[(base >> 6) + w] = make_ulonglong2(nz, neg);
+                    } else {
+                        const i64 wbase = (base - a.u_dense) >> 6;
+                        a.planes[wbase + w] = make_ulonglong2(nz, neg);
+                        a.ckpt[wbase + w] = gs[4 * w];
+                    }
                 }
             }
         }
@@ -364,14 +518,94 @@ int sieve_items_prefix(const uint4* items, int n_items, int n_primes) {
     return k;
 }
 
-void sieve_kernel_attrs(size_t smem, int block, int* per_sm) {
-    cudaFuncSetAttribute(sieve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+void sieve_kernel_attrs(size_t smem, bool odd, int block, int* per_sm) {
     *per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, sieve_kernel, block, smem);
+    if (odd) {
+        cudaFuncSetAttribute(sieve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, sieve_kernel<true>, block, smem);
+    } else {
+        cudaFuncSetAttribute(sieve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, sieve_kernel<false>, block, smem);
+    }
 }
 
-void launch_sieve(const SieveArgs& a, int grid, int block, size_t smem, cudaStream_t s) {
-    sieve_kernel<<<grid, block, smem, s>>>(a);
+void launch_sieve(const SieveArgs& a, bool odd, int grid, int block, size_t smem, cudaStream_t s) {
+    if (a.seg_end <= a.seg_begin) return;
+    if (odd) sieve_kernel<true><<<grid, block, smem, s>>>(a);
+    else sieve_kernel<false><<<grid, block, smem, s>>>(a);
+}
+
+namespace {
+// segment holding value v (1 <= v <= u_total)
+i64 segment_of_value(i64 v, i64 dense_segs, i64 u_dense, int S) {
+    return v <= u_dense ? (v - 1) / S : dense_segs + (v - 1 - u_dense) / S;
+}
+}  // namespace
+
+i64 sieve_odd_range_end(i64 a, i64 nseg, i64 dense_segs, i64 u_dense, i64 u_total, int S) {
+    // the halves of segment s reach value floor(end_s / 2); that bound grows with s
+    i64 b = a;
+    while (b < nseg) {
+        const bool dense = b < dense_segs;
+        const i64 base = dense ? b * (i64)S : u_dense + (b - dense_segs) * (i64)S;
+        const i64 end = std::min(base + (i64)S, dense ? u_dense : u_total);
+        if (segment_of_value(end / 2, dense_segs, u_dense, S) >= a) break;
+        ++b;
+    }
+    return b;
+}
+
+bool sieve_odd_ok(i64 u_dense, i64 nseg, i64 first_odd) { return (u_dense % 64) == 0 && nseg > first_odd; }
+
+// 4 copies of the periodic stencil shifted by 0..3 bytes (entry i describes
+// n = i + 1: weights of 2,3,5,7,11 and square flags of 4 and 9).
+std::vector<uint32_t> make_stencil4() {
+    std::vector<uint8_t> st(kStencilPeriod + 8);
+    const unsigned small[5] = {2, 3, 5, 7, 11};
+    for (int i = 0; i < kStencilPeriod + 8; ++i) {
+        const int n = (i % kStencilPeriod) + 1;
+        unsigned a = 0;
+        for (unsigned p : small)
+            if (n % (int)p == 0) a += (unsigned)((32 - __builtin_clz(p - 1)) | 1);
+        if (n % 4 == 0 || n % 9 == 0) a |= 0x80u;
+        st[(size_t)i] = (uint8_t)a;
+    }
+    std::vector<uint32_t> out((size_t)4 * kStencilWords);
+    for (int s = 0; s < 4; ++s)
+        for (int w = 0; w < kStencilWords; ++w) {
+            uint32_t v = 0;
+            for (int b = 0; b < 4; ++b) {
+                const size_t idx = (size_t)(4 * w + s + b);
+                v |= (uint32_t)(idx < st.size() ? st[idx] : 0) << (8 * b);
+            }
+            out[(size_t)s * kStencilWords + (size_t)w] = v;
+        }
+    return out;
+}
+
+// The same for the odd values: entry k describes n = 2k + 1 (mod 2 * 3465).
+std::vector<uint32_t> make_stencil_odd4() {
+    std::vector<uint8_t> st(kStencilOddPeriod + 8);
+    const unsigned small[4] = {3, 5, 7, 11};
+    for (int k = 0; k < kStencilOddPeriod + 8; ++k) {
+        const int n = 2 * (k % kStencilOddPeriod) + 1;
+        unsigned a = 0;
+        for (unsigned p : small)
+            if (n % (int)p == 0) a += (unsigned)((32 - __builtin_clz(p - 1)) | 1);
+        if (n % 9 == 0) a |= 0x80u;
+        st[(size_t)k] = (uint8_t)a;
+    }
+    std::vector<uint32_t> out((size_t)4 * kStencilOddWords);
+    for (int s = 0; s < 4; ++s)
+        for (int w = 0; w < kStencilOddWords; ++w) {
+            uint32_t v = 0;
+            for (int b = 0; b < 4; ++b) {
+                const size_t idx = (size_t)(4 * w + s + b);
+                v |= (uint32_t)(idx < st.size() ? st[idx] : 0) << (8 * b);
+            }
+            out[(size_t)s * kStencilOddWords + (size_t)w] = v;
+        }
+    return out;
 }
 
 // segment of value n (1 <= n <= u_total) and its position there (dense segments

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "dr_device.cuh"
@@ -10,10 +11,23 @@ namespace drb {
 
 constexpr int kStencilPeriod = 13860;                       // lcm(4, 9, 5, 7, 11)
 constexpr int kStencilWords = (kStencilPeriod + 3 + 3) / 4;  // words per shifted copy
+// Odd-value stencil: entry k describes the odd n = 2k + 1 (mod 2 * 3465): weights of
+// 3, 5, 7, 11 and the square flag of 9 (lcm(9, 5, 7, 11) = 3465 odd values).
+constexpr int kStencilOddPeriod = 3465;
+constexpr int kStencilOddWords = (kStencilOddPeriod + 3 + 3) / 4;
 
+// The sieve runs in two modes over the same segments of S values.  Full mode
+// sieves every value of a segment.  Odd mode sieves its odd values only (half the
+// marks, stencil and finalisation) and takes each even value from the Mobius bits
+// of its half, mu(2m) = -mu(m) for odd m and 0 for even m, read from the 64-value
+// plane words of the values <= u_total / 2 that earlier launches wrote: the
+// compressed planes above u_dense and the scratch planes `dplanes` below it.  A
+// launch covers segments [seg_begin, seg_end); odd-mode launches are ordered so that
+// every half they read lies in segments of earlier launches.
 struct SieveArgs {
     i64 u_total, u_dense, mu_limit;
     i64 dense_segs, nseg;
+    i64 seg_begin, seg_end;  // segments of this launch
     int S;              // values per segment (multiple of 4096)
     int n_primes;       // primes <= isqrt(u_total), ascending
     int sq_first;       // first prime >= 5 (square flags)
@@ -29,7 +43,10 @@ struct SieveArgs {
     int sqC_first;             // first prime whose square is bucketed (p^2 > S); n_primes: none
     const u64* sq_off;         // [nseg + 1]: bucketed square hits of each segment (NULL: no bucket)
     const uint32_t* sq_pos;    // their positions within the segment
-    const uint32_t* stencil4;  // 4 copies shifted by 0..3 bytes, kStencilWords each
+    const uint32_t* stencil4;  // 4 copies shifted by 0..3 bytes, kStencilWords each (full mode)
+    const uint32_t* stencil_odd4;  // the same for the odd-value stencil, kStencilOddWords each
+    ulonglong2* dplanes;       // {nonzero, negative} plane words of the values <= u_dense
+                               // (64 per word; NULL: not written, odd mode unavailable)
     int16_t* dM;
     ulonglong2* planes;
     int32_t* ckpt;
@@ -80,7 +97,7 @@ struct SumsArgs {
     i64 invw_count;
 };
 
-void launch_sieve(const SieveArgs& a, int grid, int block, size_t smem, cudaStream_t s);
+void launch_sieve(const SieveArgs& a, bool odd, int grid, int block, size_t smem, cudaStream_t s);
 // Bucketed squares: the multiples m*p^2 <= u_total of the primes p = primes[first..n)
 // (p^2 > S: at most one per segment), counted per segment, then written per segment
 // in the order of off = exclusive scan of the counts (cur: zeroed cursors).
@@ -99,7 +116,7 @@ constexpr int kMaxSieveItems = 2048;
 int build_sieve_items(const uint32_t* primes, int n_primes, int S, uint4* out, int cap);
 // Number of leading items whose prime index is below n_primes.
 int sieve_items_prefix(const uint4* items, int n_items, int n_primes);
-size_t sieve_smem_bytes(int S);
+size_t sieve_smem_bytes(int S, bool odd);
 void launch_seg_scan(const int32_t* in, int32_t* out, i64 n, cudaStream_t s);
 void launch_fixup(int16_t* dM, i64 u_dense, int S, const int32_t* seg_off, int32_t* ckpt, i64 nwords,
                   i64 dense_segs, int sm_count, cudaStream_t s);
@@ -122,7 +139,14 @@ void init_piece_constants();
 int record_error(int code, const char* msg);
 // Opt the sieve kernel into `smem` bytes of dynamic shared memory and report
 // how many CTAs of `block` threads fit on one SM.
-void sieve_kernel_attrs(size_t smem, int block, int* per_sm);
+void sieve_kernel_attrs(size_t smem, bool odd, int block, int* per_sm);
+// Segments [a, b) of an odd-mode launch that may follow launches covering [0, a):
+// the largest b such that the halves of every value of [a, b) lie below segment a.
+i64 sieve_odd_range_end(i64 a, i64 nseg, i64 dense_segs, i64 u_dense, i64 u_total, int S);
+// Whether odd mode applies: value words aligned at u_dense and enough segments.
+bool sieve_odd_ok(i64 u_dense, i64 nseg, i64 first_odd);
+std::vector<uint32_t> make_stencil4();
+std::vector<uint32_t> make_stencil_odd4();
 void sums_kernel_occupancy(int block, int* per_sm);
 void launch_debug_udiv(const u64* y, const u64* d, u64* q, i64 n, int rcp, cudaStream_t s);
 void launch_debug_piece(const int32_t* piece, const u64* q, i64* out, i64 n, int fast, cudaStream_t s);

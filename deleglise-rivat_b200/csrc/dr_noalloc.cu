@@ -137,7 +137,7 @@ void setup_device(int device, DeviceSetup& d) {
         d.status = noalloc_fail(DR_ERR_CUDA, "cudaDeviceGetAttribute failed", e);
         return;
     }
-    sieve_kernel_attrs(sieve_smem_bytes(kNoAllocSeg), 1024, &d.sieve_per_sm);
+    sieve_kernel_attrs(sieve_smem_bytes(kNoAllocSeg, false), false, 1024, &d.sieve_per_sm);
     if (d.sieve_per_sm < 1) d.sieve_per_sm = 1;
     d.status = DR_OK;
 }
@@ -197,6 +197,10 @@ extern "C" int dr_table_build_noalloc(int device, void* stream, int64_t u_total,
         a.mu_limit = mu_limit;
         a.dense_segs = dense_segs;
         a.nseg = nseg;
+        a.seg_begin = 0;  // every segment in full mode: no scratch for the dense tier's planes
+        a.seg_end = nseg;
+        a.dplanes = nullptr;
+        a.stencil_odd4 = nullptr;
         a.S = S;
         a.n_primes = count_primes_upto(root);
         a.sq_first = std::min(a.n_primes, count_primes_upto(4));
@@ -225,7 +229,7 @@ extern "C" int dr_table_build_noalloc(int device, void* stream, int64_t u_total,
         // scratch that this call reads it also writes first
         e = cudaMemsetAsync(wheel, 0, (size_t)wheel_groups * 16, s);
         if (e == cudaSuccess) {
-            launch_sieve(a, grid, 1024, sieve_smem_bytes(S), s);
+            launch_sieve(a, false, grid, 1024, sieve_smem_bytes(S, false), s);
             launch_seg_scan(a.seg_sum, seg_off, nseg, s);
             launch_fixup(dM, u_dense, S, seg_off, ckpt, nwords, dense_segs, d.sm_count, s);
             e = cudaGetLastError();
