@@ -128,18 +128,19 @@ inline void ref_compressed_params(int64_t X, dr_params* p) {
     p->mu_limit = std::min(u_total, mu_limit);
 }
 
-// B200 policy (DR_POLICY_GPU), fitted to a sweep of measured device times over
-// X = 10^14 .. 10^18 (fx in 0.15 .. 1, cx in 1 .. 2.1; table build ~3 ms per 10^9
-// values, S1 ~1.3 ms per 10^9 lookups, S2 ~3 ms per 10^9 wheel positions): the
-// table is far cheaper to build on the GPU than on the CPU, so u is raised to
-// 0.6 (X / ln ln X)^(2/3) -- the reference's u formula without its 8e9 cap --
-// and cx = 1.3.  u is capped at 2.5e11 values (~80 GB of compressed tier) and
+// B200 policy (DR_POLICY_GPU), fitted to sweeps of measured device times over
+// X = 10^14 .. 10^18 (fx in 0.15 .. 1.3, cx in 1 .. 2.1; table build ~1.3 ms per
+// 10^9 values with the odd-value sieve, S1 ~1.2 ms per 10^9 lookups, S2 ~1.9 ms
+// per 10^9 wheel positions): the table is far cheaper to build on the GPU than on
+// the CPU, so u is raised to 0.9 (X / ln ln X)^(2/3) -- the reference's u formula
+// without its 8e9 cap -- and cx = 1.3 (the optimum is flat: fx 0.75 .. 1.1 within
+// 1.5% at X = 10^16).  u is capped at 2.5e11 values (~80 GB of compressed tier) and
 // never below the endpoints; the dense tier holds max(1.28e8, u/16) values (<= 4e9).
 inline void gpu_params(int64_t X, dr_params* p) {
     params_clear(p);
     const double cx = 1.3;
     const double loglogX = std::log(std::max(2.0, std::log((double)X)));
-    int64_t u = (int64_t)(0.6 * std::pow((double)X / loglogX, 2.0 / 3.0));
+    int64_t u = (int64_t)(0.9 * std::pow((double)X / loglogX, 2.0 / 3.0));
     const int64_t S = isqrt_i64(X);
     u = std::max(u, 3 * S);
     u = std::min<int64_t>(u, 250000000000LL);
@@ -147,8 +148,8 @@ inline void gpu_params(int64_t X, dr_params* p) {
     int64_t endpoint = (int64_t)(cx * std::sqrt((double)X)) + 1000;
     u = std::max(u, std::max(S + 1000, endpoint));
     endpoint = (endpoint + 255) & ~255LL;
-    // dense int16 tier: at least the reference's 1.28e8 and u/16 (at most 4e9): a larger
-    // tier lets the windowed S1 take more lookups (measured: ~1% at X = 10^16..10^18)
+    // dense int16 tier: at least the reference's 1.28e8 and u/16 (at most 4e9); S1 lookups
+    // below it take one 2-byte gather instead of a plane word and a checkpoint
     const int64_t dense_target = std::min<int64_t>(4000000000LL, std::max<int64_t>(128000000LL, u / 16));
     const int64_t u_dense = std::min<int64_t>(u, std::max<int64_t>(endpoint, (dense_target + 255) & ~255LL));
     const int64_t N = X / u;

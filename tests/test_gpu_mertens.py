@@ -93,7 +93,7 @@ def test_bad_params_raise(engine):
 
 
 def test_gpu_policy_known_answers(engine):
-    # the B200 policy (larger u, cx = 1.2) gives the same exact values
+    # the B200 policy (larger u, cx = 1.3) gives the same exact values
     for c in load_golden("kat.json")["cases"]:
         p = dr_b200.default_params(c["X"], dr_b200.POLICY_GPU)
         assert dr_b200.check_params(c["X"], p) == 0
