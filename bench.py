@@ -356,8 +356,8 @@ def run_engine(args, world, rank, local):
     achieved = alg / (sums / 1e3) / 1e9
     # DRAM traffic: ncu dram__bytes_read.sum + dram__bytes_write.sum of sums_kernel
     # in a 1-pass capture of M(10^16) with these parameters (profiles/launches_m1e16.md):
-    # 91.9 GB for 5.33e10 ops = 1.72 B per op, times this call's op count.
-    traffic = 1.72 * (s0_.s1_ops + s0_.s2_ops)
+    # 87.2 GB for 4.35e10 ops = 2.0 B per op, times this call's op count.
+    traffic = 2.0 * (s0_.s1_ops + s0_.s2_ops)
     line = {
         "metric": "sec per M(10^16)" if X == X_HEADLINE else f"sec per M({X})", "value": value, "unit": "s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_per * 1e3,
