@@ -201,6 +201,29 @@ KNOWN = {10**k: m for k, m in [(9, -222), (10, -33722), (11, -87856), (12, 62366
                                     (15, -3216373), (16, -3195437), (17, -21830254)]}  # test_dr.cpp, test_cuda.cu, README
 
 
+def sieve_marks(u_total, u_dense, sm_count, S=1 << 17):
+    """Shared-memory atomics the table build issues: one per multiple of a prime
+    13 <= p <= sqrt(u) (log weight) and per multiple of p^2, p >= 5 (square flag),
+    every multiple in the first wave of full-mode segments (sm_count segments of S
+    values) and the odd multiples above it (odd mode, when u_dense is on a 64-value
+    word).  Counted on the host from the primes."""
+    import numpy as np
+
+    r = int(np.sqrt(u_total)) + 1
+    sieve = np.ones(r + 1, dtype=bool)
+    sieve[:2] = False
+    for i in range(2, int(r ** 0.5) + 1):
+        if sieve[i]:
+            sieve[i * i::i] = False
+    pr = np.nonzero(sieve)[0].astype(np.int64)
+    pr = pr[pr * pr <= u_total]
+    vf = min(u_total, sm_count * S) if u_dense % 64 == 0 else u_total
+    mods = np.concatenate([pr[pr >= 13], pr[pr >= 5] ** 2])
+    full = vf // mods
+    odd = (u_total // mods + 1) // 2 - (vf // mods + 1) // 2
+    return int(full.sum() + odd.sum())
+
+
 def run_table_only(args, eng, stream):
     """Time the table build alone (sieve + prefix + compressed tier): --table u_total[,u_dense[,mu_limit]]."""
     import torch
@@ -271,6 +294,9 @@ def run_engine(args, world, rank, local):
         host = max_over_ranks(host_dt, world) / steps
         return dev, host, stats
 
+    # ceilings of the units the kernels are bound by (shared atomics, IMAD, DFMA),
+    # measured here on this GPU before anything is timed
+    peaks_int = dr_b200.measure_peaks(local)
     # warm-up (also the correctness gate)
     for _ in range(args.warmup):
         check(eng.mertens(X, tuned).M)
@@ -358,6 +384,21 @@ def run_engine(args, world, rank, local):
     # in a 1-pass capture of M(10^16) with these parameters (profiles/launches_m1e16.md):
     # 87.2 GB for 4.35e10 ops = 2.0 B per op, times this call's op count.
     traffic = 2.0 * (s0_.s1_ops + s0_.s2_ops)
+    # Table build: shared-memory atomic marks issued by the sieve per second against the
+    # measured ceiling, and the table's HBM writes against the copy peak.
+    marks = sieve_marks(tuned.u_total, tuned.u_dense, torch.cuda.get_device_properties(local).multi_processor_count)
+    tbytes = 2 * tuned.u_dense + 0.3125 * (tuned.u_total - tuned.u_dense) + tuned.mu_limit / 4
+    table_roofline = {
+        "kernel": "sieve_kernel (whole table phase: sieve, bucket, scan and fixup launches)",
+        "bound": "shared-memory atomics / integer issue", "marks": marks,
+        "achieved": marks / (tab / 1e3), "peak": peaks_int["smem_atomic_per_s"],
+        "peak_sieve_pattern": peaks_int["smem_atomic_stride_per_s"], "unit": "atomics/s",
+        "frac": marks / (tab / 1e3) / peaks_int["smem_atomic_per_s"],
+        "frac_of_sieve_pattern": marks / (tab / 1e3) / peaks_int["smem_atomic_stride_per_s"],
+        "hbm": {"bytes": tbytes, "achieved": tbytes / (tab / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                "frac": tbytes / (tab / 1e3) / 1e9 / peak},
+        "peak_kind": "measured on this GPU by dr_measure_peaks (synthetic kernels)",
+    }
     line = {
         "metric": "sec per M(10^16)" if X == X_HEADLINE else f"sec per M({X})", "value": value, "unit": "s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_per * 1e3,
@@ -380,6 +421,8 @@ def run_engine(args, world, rank, local):
                      "ops": {"s1_lookups": s0_.s1_ops, "s2_positions": s0_.s2_ops},
                      "note": "sums_kernel: far S1 lookups cost a random DRAM sector each (1.3 TB/s of 32 B sectors), near ones and the S2 wheel stream hit L2; issue 57% active; ops_per_s = S1 lookups + S2 positions per second",
                      "ops_per_s": (s0_.s1_ops + s0_.s2_ops) / (sums / 1e3)},
+        "table_roofline": table_roofline,
+        "int_peaks": peaks_int,
         "clocks": clocks.summary(),
         "batched": batch,
     }

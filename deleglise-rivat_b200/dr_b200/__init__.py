@@ -156,6 +156,7 @@ def lib():
             "dr_tuner_features": (i32, [i64, u64, i32, i32, ctypes.POINTER(ctypes.c_float)]),
             "dr_tuner_params": (i32, [i64, ctypes.POINTER(ctypes.c_float), P]),
             "dr_tuner_propose": (i32, [vp, i64, u64, i32, i32, P, ctypes.POINTER(i32)]),
+            "dr_measure_peaks": (i32, [i32, ctypes.POINTER(Peaks)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -176,7 +177,21 @@ def exported_symbols() -> list:
         "dr_table_build_noalloc", "dr_autotune_batch",
         "dr_mlp_create", "dr_mlp_destroy", "dr_mlp_num_params", "dr_mlp_set_weights", "dr_mlp_get_weights",
         "dr_mlp_forward", "dr_mlp_grad", "dr_mlp_train", "dr_tuner_features", "dr_tuner_params", "dr_tuner_propose",
+        "dr_measure_peaks",
     ]
+
+
+class Peaks(ctypes.Structure):
+    """dr_peaks: measured ceilings, operations per second over the whole GPU."""
+    _fields_ = [("smem_atomic_per_s", ctypes.c_double), ("smem_atomic_stride_per_s", ctypes.c_double),
+                ("imad_per_s", ctypes.c_double), ("dfma_per_s", ctypes.c_double)]
+
+
+def measure_peaks(device: int = 0) -> dict:
+    """Shared-memory atomic, IMAD and DFMA throughput ceilings of `device` (dr_measure_peaks)."""
+    pk = Peaks()
+    _check(lib().dr_measure_peaks(int(device), ctypes.byref(pk)))
+    return {name: getattr(pk, name) for name, _ in Peaks._fields_}
 
 
 def _check(rc: int):

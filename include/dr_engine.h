@@ -179,6 +179,22 @@ int dr_debug_piece(dr_ctx *ctx, const int32_t *piece, const uint64_t *q, int64_t
 int dr_debug_udiv32(dr_ctx *ctx, const uint64_t *y, const uint64_t *d, int64_t n, uint64_t *q);
 int dr_debug_piece32(dr_ctx *ctx, const int32_t *piece, const uint64_t *q, int64_t n, int64_t *out);
 
+/* Measured throughput ceilings of the units this engine's kernels are bound by
+ * (measurement support for bench.py; no counterpart in the reference).  Each is
+ * the best of three timed launches of a synthetic kernel on `device`, in
+ * operations per second over the whole GPU: 32-bit shared-memory atomicAdd with
+ * the 32 lanes of an instruction on distinct banks (the sieve's marks), the same
+ * with the sieve's own address pattern (lane l at byte j + l*m, m odd), 32-bit
+ * integer multiply-add, and FP64 fused multiply-add.  Allocates a few KB of
+ * device memory and synchronises its own stream; takes ~0.1 s. */
+typedef struct dr_peaks {
+    double smem_atomic_per_s;
+    double smem_atomic_stride_per_s;
+    double imad_per_s;
+    double dfma_per_s;
+} dr_peaks;
+int dr_measure_peaks(int device, dr_peaks *out);
+
 /* Table build that allocates nothing.  It has no counterpart in the reference.
  *
  * For callers that cannot call cudaMalloc/cudaFree: code whose device memory

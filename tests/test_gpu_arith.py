@@ -9,6 +9,8 @@ import random
 
 import pytest
 
+import dr_b200
+
 pytestmark = pytest.mark.gpu
 
 
@@ -163,3 +165,14 @@ def test_pieces32_match_oracle(engine, oracle):
     for p, q, g in zip(pieces, vals, got):
         assert g == oracle.piece(p, q), (p, q, g)
     assert engine.debug_piece([1, 8], [2**31, 2**40], fast=True) == [-(2**63)] * 2
+
+
+def test_measure_peaks_plausible():
+    # the ceilings bench.py divides by: positive, finite and in the range a B200's
+    # units allow (148 SMs at up to ~2 GHz); the conflict-free atomic pattern is the
+    # faster one
+    pk = dr_b200.measure_peaks(0)
+    assert 1e11 < pk["smem_atomic_per_s"] < 1e14, pk
+    assert 1e10 < pk["smem_atomic_stride_per_s"] <= 1.1 * pk["smem_atomic_per_s"], pk
+    assert 1e12 < pk["imad_per_s"] < 1e14, pk
+    assert 1e11 < pk["dfma_per_s"] < 1e14, pk
