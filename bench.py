@@ -386,7 +386,8 @@ def run_engine(args, world, rank, local):
     traffic = 2.0 * (s0_.s1_ops + s0_.s2_ops)
     # Table build: shared-memory atomic marks issued by the sieve per second against the
     # measured ceiling, and the table's HBM writes against the copy peak.
-    marks = sieve_marks(tuned.u_total, tuned.u_dense, torch.cuda.get_device_properties(local).multi_processor_count)
+    marks = sieve_marks(tuned.u_total, tuned.u_dense, torch.cuda.get_device_properties(local).multi_processor_count,
+                        1 << (tuned.segment_log2 or 17))
     tbytes = 2 * tuned.u_dense + 0.3125 * (tuned.u_total - tuned.u_dense) + tuned.mu_limit / 4
     table_roofline = {
         "kernel": "sieve_kernel (whole table phase: sieve, bucket, scan and fixup launches)",

@@ -240,7 +240,7 @@ int64_t split_point_host(double cx, int64_t y) {
 
 int pick_segment(const dr_params* p) {
     int lg = (p && p->segment_log2) ? p->segment_log2 : 17;
-    lg = std::max(12, std::min(lg, 17));
+    lg = std::max(12, std::min(lg, 18));
     return 1 << lg;
 }
 
@@ -313,6 +313,7 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     a.dense_segs = dense_segs;
     a.nseg = nseg;
     a.S = S;
+    a.S_sub = std::min(S, kSieveFullPass);
     a.n_primes = (int)pr.size();
     auto first_at_least = [&](uint32_t v) {
         return (int)(std::lower_bound(pr.begin(), pr.end(), v) - pr.begin());
@@ -339,7 +340,7 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
         m.items = (const uint4*)buf.p;
         return DR_OK;
     };
-    if ((rc = set_moduli(a, S, c->items))) return rc;
+    if ((rc = set_moduli(a, a.S_sub, c->items))) return rc;
     a.primes = (const uint32_t*)c->primes.p;
     a.pinv = (const u64*)c->pinv.p;
     a.sqinv = (const u64*)c->pinv.p + pr.size();
@@ -1109,7 +1110,7 @@ int dr_autotune_batch(dr_ctx* c, const int64_t* X, int64_t count, int max_trials
     best_state = cur;
     const double ms[] = {0.25, 0.5, 2.0, 4.0, 8.0, 16.0};
     const double cxs[] = {0.9, 1.05, 1.4, 1.7};
-    const int segs[] = {15, 16};
+    const int segs[] = {15, 16, 18};
     const int blocks[] = {512};
     const int chunks[] = {12, 14, 16};
     for (int pass = 0; pass < 2 && trials < max_trials; ++pass) {

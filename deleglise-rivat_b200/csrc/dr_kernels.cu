@@ -98,11 +98,13 @@ __device__ __forceinline__ uint32_t finalize_byte(uint32_t acc, u64 n) {
     return (odd == sieved_all) ? 0xFFu : 1u;
 }
 
-// Shared memory of a sieve CTA.  Full mode: the S-byte segment and 16-value group
-// sums.  Odd mode: S/2 bytes (the odd values), 64-value word sums and plane words.
+// Shared memory of a sieve CTA.  Full mode: a pass of min(S, 2^17) bytes and its
+// 16-value group sums.  Odd mode: S/2 bytes (the odd values), 64-value word sums and
+// plane words.
 size_t sieve_smem_bytes(int S, bool odd) {
-    return odd ? (size_t)S / 2 + (size_t)(S / 64) * 4 + (size_t)(S / 64) * 16 + 64
-               : (size_t)S + (size_t)(S / 16) * 4 + 64;
+    const int B = odd ? S : std::min(S, kSieveFullPass);
+    return odd ? (size_t)B / 2 + (size_t)(B / 64) * 4 + (size_t)(B / 64) * 16 + 64
+               : (size_t)B + (size_t)(B / 16) * 4 + 64;
 }
 
 // {nonzero, negative} plane words of 64 consecutive mu bytes src[16w .. 16w+16)
@@ -215,7 +217,7 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint8_t* buf = smem;
     uint32_t* buf32 = reinterpret_cast<uint32_t*>(smem);
-    int32_t* gs = reinterpret_cast<int32_t*>(smem + (ODD ? a.S / 2 : a.S));
+    int32_t* gs = reinterpret_cast<int32_t*>(smem + (ODD ? a.S / 2 : a.S_sub));
     ulonglong2* wpl = reinterpret_cast<ulonglong2*>(smem + a.S / 2 + (a.S / 64) * 4);  // ODD only
     __shared__ int32_t wtot[33];
 
@@ -223,8 +225,14 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
 
     for (i64 seg = a.seg_begin + blockIdx.x; seg < a.seg_end; seg += gridDim.x) {
         const bool dense = seg < a.dense_segs;
-        const i64 base = dense ? seg * (i64)a.S : a.u_dense + (seg - a.dense_segs) * (i64)a.S;
-        const i64 end = min(base + (i64)a.S, dense ? a.u_dense : a.u_total);
+        const i64 seg_base = dense ? seg * (i64)a.S : a.u_dense + (seg - a.dense_segs) * (i64)a.S;
+        const i64 seg_end = min(seg_base + (i64)a.S, dense ? a.u_dense : a.u_total);
+        // Full mode sieves a segment in passes of S_sub values (the shared buffer holds
+        // S_sub bytes), carrying the Mobius sum of the earlier passes into the outputs.
+        const i64 pass_len = ODD ? (i64)a.S : (i64)a.S_sub;
+        int carry = 0;
+      for (i64 base = seg_base; base < seg_end; base += pass_len) {
+        const i64 end = min(base + pass_len, seg_end);
         const int len = (int)(end - base);
         const i64 low = base + 1;
         // sieved bytes: value low + j (full) or the odd value low + 2j (ODD; low is odd)
@@ -292,8 +300,11 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
         }
         if (a.sq_off) {
             const u64 h1 = __ldg(a.sq_off + seg + 1);
+            const uint32_t off = (uint32_t)(base - seg_base);  // this pass's first offset
             for (u64 h = __ldg(a.sq_off + seg) + tid; h < h1; h += T) {
-                uint32_t j = __ldg(a.sq_pos + h);
+                uint32_t j = __ldg(a.sq_pos + h);  // offset in the segment
+                if (j < off || j - off >= (uint32_t)len) continue;
+                j -= off;
                 if (ODD) {
                     if (j & 1u) continue;  // even value
                     j >>= 1;
@@ -409,7 +420,7 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
                     const int w = g >> 2, sub = g & 3;
                     const ulonglong2 P = wpl[w];
                     const u64 below = sub ? (1ull << (16 * sub)) - 1 : 0ull;
-                    int run = gs[w] + __popcll(P.x & below) - 2 * __popcll(P.y & below);
+                    int run = carry + gs[w] + __popcll(P.x & below) - 2 * __popcll(P.y & below);
                     const uint32_t z = (uint32_t)(P.x >> (16 * sub)) & 0xFFFFu;
                     const uint32_t n = (uint32_t)(P.y >> (16 * sub)) & 0xFFFFu;
                     uint32_t pk[8];
@@ -431,7 +442,7 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
                 }
             } else {
                 int32_t* ck = a.ckpt + ((base - a.u_dense) >> 6);
-                for (int w = tid; w < nwords; w += T) ck[w] = gs[w];
+                for (int w = tid; w < nwords; w += T) ck[w] = carry + gs[w];
             }
         } else {
             // 5. 16-value group sums and their exclusive scan
@@ -452,7 +463,7 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
                 int16_t* out = a.dM + base;
                 for (int g = tid; g < ng; g += T) {
                     const uint4 v = reinterpret_cast<const uint4*>(buf)[g];
-                    int run = gs[g];
+                    int run = carry + gs[g];
                     uint32_t pk[8];
                     const uint32_t words[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
@@ -483,13 +494,15 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
                     } else {
                         const i64 wbase = (base - a.u_dense) >> 6;
                         a.planes[wbase + w] = make_ulonglong2(nz, neg);
-                        a.ckpt[wbase + w] = gs[4 * w];
+                        a.ckpt[wbase + w] = carry + gs[4 * w];
                     }
                 }
             }
         }
-        if (tid == 0) a.seg_sum[seg] = total;
-        __syncthreads();
+        carry += total;
+        __syncthreads();  // the next pass reuses the shared buffer
+      }
+        if (tid == 0) a.seg_sum[seg] = carry;
     }
 }
 

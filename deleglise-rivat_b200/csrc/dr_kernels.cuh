@@ -14,6 +14,8 @@ constexpr int kStencilWords = (kStencilPeriod + 3 + 3) / 4;  // words per shifte
 // Odd-value stencil: entry k describes the odd n = 2k + 1 (mod 2 * 3465): weights of
 // 3, 5, 7, 11 and the square flag of 9 (lcm(9, 5, 7, 11) = 3465 odd values).
 constexpr int kStencilOddPeriod = 3465;
+// Values per full-mode pass: the full-mode shared buffer holds one byte per value.
+constexpr int kSieveFullPass = 1 << 17;
 constexpr int kStencilOddWords = (kStencilOddPeriod + 3 + 3) / 4;
 
 // The sieve runs in two modes over the same segments of S values.  Full mode
@@ -29,6 +31,7 @@ struct SieveArgs {
     i64 dense_segs, nseg;
     i64 seg_begin, seg_end;  // segments of this launch
     int S;              // values per segment (multiple of 4096)
+    int S_sub;          // values per full-mode pass: min(S, kSieveFullPass)
     int n_primes;       // primes <= isqrt(u_total), ascending
     int sq_first;       // first prime >= 5 (square flags)
     int w_first;        // first prime >= 13 (weights)

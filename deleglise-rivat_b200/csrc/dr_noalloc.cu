@@ -202,6 +202,7 @@ extern "C" int dr_table_build_noalloc(int device, void* stream, int64_t u_total,
         a.dplanes = nullptr;
         a.stencil_odd4 = nullptr;
         a.S = S;
+        a.S_sub = S;
         a.n_primes = count_primes_upto(root);
         a.sq_first = std::min(a.n_primes, count_primes_upto(4));
         a.w_first = std::min(a.n_primes, count_primes_upto(12));

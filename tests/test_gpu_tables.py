@@ -71,7 +71,7 @@ def test_block_shapes(engine, oracle):
     total, dense = 2000003, 300001
     _, _, so = oracle.table(total, dense, total)
     for block in (256, 512, 1024):
-        for seg_log2 in (12, 14, 16, 17):
+        for seg_log2 in (12, 14, 16, 17, 18):  # 2^18: full mode in two passes per segment
             engine.table_build(total, dense, total, dr_b200.Params(segment_log2=seg_log2, block_threads=block))
             assert engine.table_checksums() == tuple(so), (block, seg_log2)
 
@@ -81,7 +81,7 @@ def test_odd_mode_tables(engine, oracle):
     # is sieved on its odd values and takes its even ones from their halves, in
     # launches whose halves lie in earlier launches (many launches at 4096 values).
     for total, dense in [(1000033, 0), (1000033, 64 * 5000), (2000003, 300032), (4000037, 3999936)]:
-        for seg_log2 in (12, 13, 17):
+        for seg_log2 in (12, 13, 17, 18):
             _check_table(engine, oracle, total, dense, total, seg_log2)
     for block in (256, 512):
         engine.table_build(2000003, 300032, 2000003, dr_b200.Params(segment_log2=12, block_threads=block))
@@ -92,7 +92,7 @@ def test_odd_mode_tables(engine, oracle):
 def test_odd_mode_large_table(engine, oracle):
     total, dense = 300000007, 40000000
     _, _, so = oracle.table(total, dense, 5000000)
-    for seg_log2 in (12, 17):
+    for seg_log2 in (12, 17, 18):
         engine.table_build(total, dense, 5000000, dr_b200.Params(segment_log2=seg_log2))
         assert engine.table_checksums() == tuple(so), seg_log2
     M, _ = engine.table_read(total - 5000, 5001)
