@@ -239,7 +239,7 @@ int64_t split_point_host(double cx, int64_t y) {
 }
 
 int pick_segment(const dr_params* p) {
-    int lg = (p && p->segment_log2) ? p->segment_log2 : 17;
+    int lg = (p && p->segment_log2) ? p->segment_log2 : 18;
     lg = std::max(12, std::min(lg, 18));
     return 1 << lg;
 }
@@ -1088,7 +1088,7 @@ int dr_autotune_batch(dr_ctx* c, const int64_t* X, int64_t count, int max_trials
     const bool saved_graphs = c->graphs_enabled;
     c->graphs_enabled = false;  // trials run eagerly; only the winner is worth a graph
     std::vector<int64_t> res((size_t)count);
-    struct State { double m, cx; int seg, block, chunk; } cur{1.0, 1.2, 17, 1024, 0}, best_state = cur;
+    struct State { double m, cx; int seg, block, chunk; } cur{1.0, 1.2, 18, 1024, 0}, best_state = cur;
     double best = 1e300;
     int trials = 0;
     if (max_trials <= 0) max_trials = 24;
@@ -1110,7 +1110,7 @@ int dr_autotune_batch(dr_ctx* c, const int64_t* X, int64_t count, int max_trials
     best_state = cur;
     const double ms[] = {0.25, 0.5, 2.0, 4.0, 8.0, 16.0};
     const double cxs[] = {0.9, 1.05, 1.4, 1.7};
-    const int segs[] = {15, 16, 18};
+    const int segs[] = {16, 17};
     const int blocks[] = {512};
     const int chunks[] = {12, 14, 16};
     for (int pass = 0; pass < 2 && trials < max_trials; ++pass) {

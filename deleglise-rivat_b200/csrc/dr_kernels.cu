@@ -223,6 +223,22 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
 
     const int T = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = T >> 5;
 
+    // Each warp keeps its marking items -- items warp + nwarps*k, k < 32, one per lane,
+    // with the modulus reciprocal -- in registers for every segment and reads them by
+    // shuffles, instead of two dependent loads per item and segment (more items: the
+    // loop from memory below).
+    uint4 myI = make_uint4(0u, 0xFFFFFFFFu, 0u, 0u);
+    u64 myInv = 0;
+    const bool ireg = a.n_items <= 32 * nwarps;
+    {
+        const int my_it = warp + nwarps * lane;
+        if (ireg && my_it < a.n_items) {
+            myI = __ldg(a.items + my_it);
+            const uint32_t pidx = myI.w & 0x7fffffffu;
+            myInv = (myI.w >> 31) ? __ldg(a.sqinv + pidx) : __ldg(a.pinv + pidx);
+        }
+    }
+    const int my_cnt = (ireg && a.n_items > warp) ? (a.n_items - warp + nwarps - 1) / nwarps : 0;
     for (i64 seg = a.seg_begin + blockIdx.x; seg < a.seg_end; seg += gridDim.x) {
         const bool dense = seg < a.dense_segs;
         const i64 seg_base = dense ? seg * (i64)a.S : a.u_dense + (seg - a.dense_segs) * (i64)a.S;
@@ -264,13 +280,16 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
         //    the order of the marks does not matter.  ODD: the odd multiples only,
         //    consecutive ones 2m apart in value, m apart in bytes.
         //    Smaller moduli: balanced warp items (lanes stride the multiples).
-        for (int it = warp; it < a.n_items; it += nwarps) {
-            const uint4 I = __ldg(a.items + it);
+        for (int k = 0; k < (ireg ? my_cnt : 0); ++k) {
+            uint4 I;
+            I.x = __shfl_sync(0xffffffffu, myI.x, k);
+            I.y = __shfl_sync(0xffffffffu, myI.y, k);
+            I.z = __shfl_sync(0xffffffffu, myI.z, k);
+            I.w = __shfl_sync(0xffffffffu, myI.w, k);
+            const u64 inv = __shfl_sync(0xffffffffu, myInv, k);
             if (I.y >= (uint32_t)nb) continue;
             const uint32_t m = I.x;
             const bool sq = (I.w >> 31) != 0;
-            const uint32_t pidx = I.w & 0x7fffffffu;
-            const u64 inv = sq ? __ldg(a.sqinv + pidx) : __ldg(a.pinv + pidx);
             const u64 v0 = (u64)low + (ODD ? 2ull * I.y : (u64)I.y);  // value of byte I.y
             const uint32_t r = (uint32_t)umod_inv(v0, m, inv);
             uint32_t d = r ? m - r : 0u;  // first multiple: v0 + d
@@ -282,6 +301,25 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
             } else {
                 const uint32_t add = I.z;
                 for (; j < jend; j += 32u * m) atomicAdd(&buf32[j >> 2], add << ((j & 3) * 8));
+            }
+        }
+        for (int it = warp; it < (ireg ? 0 : a.n_items); it += nwarps) {
+            const uint4 I = __ldg(a.items + it);
+            if (I.y >= (uint32_t)nb) continue;
+            const uint32_t m = I.x;
+            const bool sq = (I.w >> 31) != 0;
+            const uint32_t pidx = I.w & 0x7fffffffu;
+            const u64 inv = sq ? __ldg(a.sqinv + pidx) : __ldg(a.pinv + pidx);
+            const u64 v0 = (u64)low + (ODD ? 2ull * I.y : (u64)I.y);
+            const uint32_t r = (uint32_t)umod_inv(v0, m, inv);
+            uint32_t d = r ? m - r : 0u;
+            if (ODD && (d & 1u)) d += m;
+            uint32_t j = I.y + (ODD ? d >> 1 : d) + (uint32_t)lane * m;
+            const uint32_t jend = min((uint32_t)nb, I.y + 1024u * m);
+            if (sq) {
+                for (; j < jend; j += 32u * m) atomicOr(&buf32[j >> 2], 0x80u << ((j & 3) * 8));
+            } else {
+                for (; j < jend; j += 32u * m) atomicAdd(&buf32[j >> 2], I.z << ((j & 3) * 8));
             }
         }
         //    Larger moduli (at most 32 hits per segment): one prime per thread.
@@ -315,12 +353,23 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
         //    Offsets low mod p: on the 32-bit quotient route (qest/qfix) while
         //    p <= low and low/p < 2^31, else from the 64-bit reciprocal.
         const double lowd = __ull2double_rn((u64)low);
+        uint32_t p_n = 0;
+        double rc_n = 0.0;
+        if (a.tierB_first + tid < a.n_primes) {
+            p_n = __ldg(a.primes + a.tierB_first + tid);
+            if (a.prcp) rc_n = __ldg(a.prcp + a.tierB_first + tid);
+        }
         for (int i = a.tierB_first + tid; i < a.n_primes; i += T) {
-            const uint32_t p = a.primes[i];
+            const uint32_t p = p_n;  // loaded one iteration ahead
+            const double rc = rc_n;
+            if (i + T < a.n_primes) {
+                p_n = __ldg(a.primes + i + T);
+                if (a.prcp) rc_n = __ldg(a.prcp + i + T);
+            }
             const uint32_t w = (32u - __clz(p - 1)) | 1u;
             uint32_t r;
             if (a.prcp && (u64)low >= p && ((u64)low >> 31) < p)
-                r = (uint32_t)low - qfix(qest(lowd, __ldg(a.prcp + i)), (uint32_t)low, p) * p;
+                r = (uint32_t)low - qfix(qest(lowd, rc), (uint32_t)low, p) * p;
             else
                 r = (uint32_t)umod_inv((u64)low, p, a.pinv[i]);
             uint32_t d = r ? p - r : 0;

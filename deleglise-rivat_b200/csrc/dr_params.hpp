@@ -158,9 +158,6 @@ inline void gpu_params(int64_t X, dr_params* p) {
     p->u_dense = u_dense;
     p->cx = cx;
     p->mu_limit = std::min(u, std::max(A_max, N + 1000));
-    // 2^18-value sieve segments from 2^32 values on: half the per-segment cost of the
-    // larger primes' offsets (table build -5% at X = 10^16, -13% at 10^18)
-    if (u >= (int64_t(1) << 32)) p->segment_log2 = 18;
 }
 
 }  // namespace drb
