@@ -167,8 +167,23 @@ __device__ __forceinline__ u64 spread32(uint32_t x) {
 // Even values 2m (odd b = 2k+1, m = base/2 + 32w + k + 1) from the plane bits of m:
 // mu(2m) = -mu(m) for odd m (k even), 0 for even m; the 32 values m are one aligned
 // half of a plane word (base/2 + 32w is a multiple of 32).
+//
+// Fused finalisation (fz.on): the shared words still hold the sieve's accumulator
+// bytes, and the byte-log rule of step 4 is applied here, word by word, instead of in
+// a pass of its own: a byte is nonzero iff its square flag (bit 7) is clear, negative
+// iff also bit 7 of a + k (k below or above the power-of-two edge) equals its parity
+// bit.  Word fz.skip (the one straddling the edge, if any) was finalised by step 4;
+// bytes at or past nb read as 0.
+struct FusedFinal {
+    bool on;
+    int skip;            // word index already finalised, or -1
+    int nb;              // sieved bytes
+    i64 edge;            // first byte whose value reaches the next power of two
+    uint32_t kbelow, kabove;
+};
+
 __device__ __forceinline__ void planes_odd_mode(const SieveArgs& a, const uint32_t* buf32, int w, int nw16,
-                                                int lane, i64 base, u64* nz, u64* neg) {
+                                                int lane, i64 base, const FusedFinal& fz, u64* nz, u64* neg) {
     const uint32_t rot = (uint32_t)(lane >> 2) & 7u;
     const uint32_t* src = buf32 + 8 * w;
     const bool full = 8 * w + 8 <= nw16;
@@ -176,9 +191,27 @@ __device__ __forceinline__ void planes_odd_mode(const SieveArgs& a, const uint32
 #pragma unroll
     for (int t = 0; t < 8; ++t) {
         const uint32_t tt = ((uint32_t)t + rot) & 7u;
-        const uint32_t v = (full || 8 * w + (int)tt < nw16) ? src[tt] : 0u;
-        const uint32_t z = ((v & 0x01010101u) * 0x01041040u) >> 24;         // bits 0, 2, 4, 6
-        const uint32_t g = (((v >> 7) & 0x01010101u) * 0x01041040u) >> 24;
+        const int idx = 8 * w + (int)tt;
+        const uint32_t v = (full || idx < nw16) ? src[tt] : 0u;
+        uint32_t nzb, ngb;
+        if (fz.on && idx != fz.skip) {
+            const i64 j0 = 4 * (i64)idx;
+            const uint32_t s = (v & 0x7F7F7F7Fu) + (j0 < fz.edge ? fz.kbelow : fz.kabove);
+            const uint32_t x = ((s >> 7) ^ v) & 0x01010101u;  // 1: mu = +1 (if not flagged)
+            nzb = ~(v >> 7) & 0x01010101u;
+            ngb = nzb & ~x;
+            const int rem = fz.nb - 4 * idx;
+            if (rem < 4) {
+                const uint32_t m = rem <= 0 ? 0u : (0x01010101u & ((1u << (8 * rem)) - 1u));
+                nzb &= m;
+                ngb &= m;
+            }
+        } else {
+            nzb = v & 0x01010101u;
+            ngb = (v >> 7) & 0x01010101u;
+        }
+        const uint32_t z = (nzb * 0x01041040u) >> 24;  // bits 0, 2, 4, 6
+        const uint32_t g = (ngb * 0x01041040u) >> 24;
         if (t < 4) {
             zl |= z << (8 * t);
             gl |= g << (8 * t);
@@ -387,6 +420,9 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
         //    most one power of two above its start once low >= len (bits steps
         //    there); the word straddling it, the words holding n <= 2 and the
         //    first segments take the per-byte rule.  Bytes past nb become 0.
+        //    Odd-mode segments that write no wheel bits leave this to the plane
+        //    assembly (FusedFinal) but for the word straddling the power-of-two edge.
+        FusedFinal fz;
         {
             const int bw_low = 64 - __clzll((u64)low);
             const u64 pow2 = 1ull << bw_low;  // first n above low with a larger bit width
@@ -395,7 +431,15 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
             const bool simple = (u64)low >= 3 && (u64)low >= (u64)len;
             // first byte whose value reaches pow2
             const i64 edge = ODD ? (i64)((pow2 - (u64)low + 1) >> 1) : (i64)(pow2 - (u64)low);
-            for (int i = tid; i < nw16; i += T) {
+            fz.on = ODD && simple && low > a.mu_limit;
+            fz.skip = ((edge & 3) && edge < 4 * (i64)nw16) ? (int)(edge >> 2) : -1;
+            fz.nb = nb;
+            fz.edge = edge;
+            fz.kbelow = kbelow;
+            fz.kabove = kabove;
+            const int i_first = fz.on ? (tid == 0 && fz.skip >= 0 ? fz.skip : nw16) : tid;
+            const int i_end = fz.on ? min(nw16, fz.skip + 1) : nw16;
+            for (int i = i_first; i < i_end; i += T) {
                 const uint32_t v = buf32[i];
                 const i64 j0 = 4 * (i64)i;
                 uint32_t o;
@@ -450,7 +494,7 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
             const u64 lastmask = (len & 63) ? (1ull << (len & 63)) - 1 : ~0ull;
             for (int w = tid; w < nwords; w += T) {
                 u64 nz, neg;
-                planes_odd_mode(a, buf32, w, nw16, lane, base, &nz, &neg);
+                planes_odd_mode(a, buf32, w, nw16, lane, base, fz, &nz, &neg);
                 if (w == nwords - 1) {
                     nz &= lastmask;
                     neg &= lastmask;

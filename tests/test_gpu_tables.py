@@ -83,6 +83,9 @@ def test_odd_mode_tables(engine, oracle):
     for total, dense in [(1000033, 0), (1000033, 64 * 5000), (2000003, 300032), (4000037, 3999936)]:
         for seg_log2 in (12, 13, 17, 18):
             _check_table(engine, oracle, total, dense, total, seg_log2)
+        # a small mu limit: segments above it finalise inside the plane assembly
+        for seg_log2 in (12, 18):
+            _check_table(engine, oracle, total, dense, 999, seg_log2)
     for block in (256, 512):
         engine.table_build(2000003, 300032, 2000003, dr_b200.Params(segment_log2=12, block_threads=block))
         _, _, so = oracle.table(2000003, 300032, 2000003)
