@@ -242,6 +242,26 @@ __device__ __forceinline__ void planes_odd_mode(const SieveArgs& a, const uint32
     *neg = g;
 }
 
+// Marks of one warp item I = {modulus m, first byte, weight or 0x80, prime index |
+// square bit 31}: lanes stride the multiples of m at or after byte I.y (ODD: the odd
+// multiples, m bytes apart), 32 strides each, with the 64-bit reciprocal inv of m.
+template <bool ODD>
+__device__ __forceinline__ void mark_item(uint32_t* buf32, const uint4 I, const u64 inv, i64 low, int nb,
+                                          int lane) {
+    const uint32_t m = I.x;
+    const u64 v0 = (u64)low + (ODD ? 2ull * I.y : (u64)I.y);  // value of byte I.y
+    const uint32_t r = (uint32_t)umod_inv(v0, m, inv);
+    uint32_t d = r ? m - r : 0u;  // first multiple: v0 + d
+    if (ODD && (d & 1u)) d += m;  // v0 is odd: the first odd multiple
+    uint32_t j = I.y + (ODD ? d >> 1 : d) + (uint32_t)lane * m;
+    const uint32_t jend = min((uint32_t)nb, I.y + 1024u * m);
+    if (I.w >> 31) {
+        for (; j < jend; j += 32u * m) atomicOr(&buf32[j >> 2], 0x80u << ((j & 3) * 8));
+    } else {
+        for (; j < jend; j += 32u * m) atomicAdd(&buf32[j >> 2], I.z << ((j & 3) * 8));
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Segmented byte-log Mobius sieve + table outputs (ODD: odd values only).
 // ---------------------------------------------------------------------------
@@ -319,41 +339,13 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
             I.y = __shfl_sync(0xffffffffu, myI.y, k);
             I.z = __shfl_sync(0xffffffffu, myI.z, k);
             I.w = __shfl_sync(0xffffffffu, myI.w, k);
-            const u64 inv = __shfl_sync(0xffffffffu, myInv, k);
-            if (I.y >= (uint32_t)nb) continue;
-            const uint32_t m = I.x;
-            const bool sq = (I.w >> 31) != 0;
-            const u64 v0 = (u64)low + (ODD ? 2ull * I.y : (u64)I.y);  // value of byte I.y
-            const uint32_t r = (uint32_t)umod_inv(v0, m, inv);
-            uint32_t d = r ? m - r : 0u;  // first multiple: v0 + d
-            if (ODD && (d & 1u)) d += m;  // v0 is odd: the first odd multiple
-            uint32_t j = I.y + (ODD ? d >> 1 : d) + (uint32_t)lane * m;
-            const uint32_t jend = min((uint32_t)nb, I.y + 1024u * m);
-            if (sq) {
-                for (; j < jend; j += 32u * m) atomicOr(&buf32[j >> 2], 0x80u << ((j & 3) * 8));
-            } else {
-                const uint32_t add = I.z;
-                for (; j < jend; j += 32u * m) atomicAdd(&buf32[j >> 2], add << ((j & 3) * 8));
-            }
+            if (I.y < (uint32_t)nb) mark_item<ODD>(buf32, I, __shfl_sync(0xffffffffu, myInv, k), low, nb, lane);
         }
         for (int it = warp; it < (ireg ? 0 : a.n_items); it += nwarps) {
             const uint4 I = __ldg(a.items + it);
             if (I.y >= (uint32_t)nb) continue;
-            const uint32_t m = I.x;
-            const bool sq = (I.w >> 31) != 0;
             const uint32_t pidx = I.w & 0x7fffffffu;
-            const u64 inv = sq ? __ldg(a.sqinv + pidx) : __ldg(a.pinv + pidx);
-            const u64 v0 = (u64)low + (ODD ? 2ull * I.y : (u64)I.y);
-            const uint32_t r = (uint32_t)umod_inv(v0, m, inv);
-            uint32_t d = r ? m - r : 0u;
-            if (ODD && (d & 1u)) d += m;
-            uint32_t j = I.y + (ODD ? d >> 1 : d) + (uint32_t)lane * m;
-            const uint32_t jend = min((uint32_t)nb, I.y + 1024u * m);
-            if (sq) {
-                for (; j < jend; j += 32u * m) atomicOr(&buf32[j >> 2], 0x80u << ((j & 3) * 8));
-            } else {
-                for (; j < jend; j += 32u * m) atomicAdd(&buf32[j >> 2], I.z << ((j & 3) * 8));
-            }
+            mark_item<ODD>(buf32, I, (I.w >> 31) ? __ldg(a.sqinv + pidx) : __ldg(a.pinv + pidx), low, nb, lane);
         }
         //    Larger moduli (at most 32 hits per segment): one prime per thread.
         //    Squares above S hit a segment at most once: their hits come from
