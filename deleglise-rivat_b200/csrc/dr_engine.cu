@@ -381,8 +381,9 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     sieve_kernel_attrs(smem_o, true, block, &per_o);
     const int64_t grid_f = (int64_t)c->sm_count * std::max(per_f, 1);
     const int64_t grid_o = (int64_t)c->sm_count * std::max(per_o, 1);
-    const int64_t first_odd = std::min<int64_t>(nseg, grid_f);
-    const bool odd = sieve_odd_ok(u_dense, nseg, first_odd);
+    const std::vector<SieveLaunch> plan = sieve_launch_plan(u_total, u_dense, S, grid_f);
+    bool odd = false;
+    for (const SieveLaunch& l : plan) odd = odd || l.odd;
     SieveArgs ao = a;
     if (odd) {
         if ((rc = ensure(c, c->dplanes, (size_t)(u_dense / 64 + 1) * 16))) return rc;
@@ -406,23 +407,15 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
         CU(cudaGetLastError());
         launches += 5;
     }
-    a.seg_begin = 0;
-    a.seg_end = odd ? first_odd : nseg;
-    launch_sieve(a, false, (int)std::max<int64_t>(1, std::min<int64_t>(a.seg_end, grid_f)), block, smem_f, c->stream);
-    CU(cudaGetLastError());
-    for (int64_t b0 = a.seg_end; b0 < nseg;) {
-        int64_t b1 = sieve_odd_range_end(b0, nseg, dense_segs, u_dense, u_total, S);
-        const bool use_odd = b1 > b0;
-        if (!use_odd) b1 = nseg;  // never expected: the rest in full mode
-        SieveArgs& m = use_odd ? ao : a;
-        m.seg_begin = b0;
-        m.seg_end = b1;
-        launch_sieve(m, use_odd, (int)std::min<int64_t>(b1 - b0, use_odd ? grid_o : grid_f), block,
-                     use_odd ? smem_o : smem_f, c->stream);
+    for (const SieveLaunch& l : plan) {
+        SieveArgs& m = l.odd ? ao : a;
+        m.seg_begin = l.begin;
+        m.seg_end = l.end;
+        launch_sieve(m, l.odd, (int)std::max<int64_t>(1, std::min<int64_t>(l.end - l.begin, l.odd ? grid_o : grid_f)),
+                     block, l.odd ? smem_o : smem_f, c->stream);
         CU(cudaGetLastError());
-        ++launches;
-        b0 = b1;
     }
+    launches += (int)plan.size() - 1;
     launch_seg_scan((const int32_t*)c->seg_sum.p, (int32_t*)c->seg_off.p, nseg, c->stream);
     CU(cudaGetLastError());
     launch_fixup((int16_t*)c->dM.p, u_dense, S, (const int32_t*)c->seg_off.p, (int32_t*)c->ckpt.p, nwords,
@@ -1276,6 +1269,20 @@ int dr_debug_piece(dr_ctx* c, const int32_t* piece, const uint64_t* q, int64_t n
 
 int dr_debug_piece32(dr_ctx* c, const int32_t* piece, const uint64_t* q, int64_t n, int64_t* out) {
     return debug_piece(c, piece, q, n, out, 1);
+}
+
+int64_t dr_debug_sieve_plan(int64_t u_total, int64_t u_dense, int32_t segment_log2, int64_t first_wave,
+                            int64_t* out, int64_t cap) {
+    if (u_total < 1 || u_dense < 0 || u_dense > u_total || segment_log2 < 12 || segment_log2 > 18 || first_wave < 1 ||
+        cap < 0 || (cap > 0 && !out))
+        return fail(DR_ERR_ARG, "dr_debug_sieve_plan: bad arguments");
+    const std::vector<SieveLaunch> plan = sieve_launch_plan(u_total, u_dense, 1 << segment_log2, first_wave);
+    for (size_t i = 0; i < plan.size() && (int64_t)i < cap; ++i) {
+        out[3 * i] = plan[i].begin;
+        out[3 * i + 1] = plan[i].end;
+        out[3 * i + 2] = plan[i].odd ? 1 : 0;
+    }
+    return (int64_t)plan.size();
 }
 
 }  // extern "C"

@@ -655,6 +655,28 @@ i64 sieve_odd_range_end(i64 a, i64 nseg, i64 dense_segs, i64 u_dense, i64 u_tota
 
 bool sieve_odd_ok(i64 u_dense, i64 nseg, i64 first_odd) { return (u_dense % 64) == 0 && nseg > first_odd; }
 
+std::vector<SieveLaunch> sieve_launch_plan(i64 u_total, i64 u_dense, int S, i64 first_wave) {
+    const i64 dense_segs = (u_dense + S - 1) / S;
+    const i64 nseg = dense_segs + (u_total - u_dense + S - 1) / S;
+    const i64 first_odd = std::min<i64>(nseg, std::max<i64>(first_wave, 1));
+    std::vector<SieveLaunch> plan;
+    if (!sieve_odd_ok(u_dense, nseg, first_odd)) {
+        plan.push_back({0, nseg, false});
+        return plan;
+    }
+    plan.push_back({0, first_odd, false});
+    for (i64 b0 = first_odd; b0 < nseg;) {
+        const i64 b1 = sieve_odd_range_end(b0, nseg, dense_segs, u_dense, u_total, S);
+        if (b1 <= b0) {  // never expected: the rest in full mode
+            plan.push_back({b0, nseg, false});
+            break;
+        }
+        plan.push_back({b0, b1, true});
+        b0 = b1;
+    }
+    return plan;
+}
+
 // 4 copies of the periodic stencil shifted by 0..3 bytes (entry i describes
 // n = i + 1: weights of 2,3,5,7,11 and square flags of 4 and 9).
 std::vector<uint32_t> make_stencil4() {

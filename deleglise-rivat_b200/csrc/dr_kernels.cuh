@@ -148,6 +148,14 @@ void sieve_kernel_attrs(size_t smem, bool odd, int block, int* per_sm);
 i64 sieve_odd_range_end(i64 a, i64 nseg, i64 dense_segs, i64 u_dense, i64 u_total, int S);
 // Whether odd mode applies: value words aligned at u_dense and enough segments.
 bool sieve_odd_ok(i64 u_dense, i64 nseg, i64 first_odd);
+// The sieve launches of a table build, in stream order: the first wave of
+// first_wave segments in full mode, then odd-mode ranges from sieve_odd_range_end
+// (or everything in full mode where odd mode does not apply).
+struct SieveLaunch {
+    i64 begin, end;
+    bool odd;
+};
+std::vector<SieveLaunch> sieve_launch_plan(i64 u_total, i64 u_dense, int S, i64 first_wave);
 std::vector<uint32_t> make_stencil4();
 std::vector<uint32_t> make_stencil_odd4();
 void sums_kernel_occupancy(int block, int* per_sm);

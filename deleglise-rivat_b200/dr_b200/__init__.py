@@ -157,6 +157,7 @@ def lib():
             "dr_tuner_params": (i32, [i64, ctypes.POINTER(ctypes.c_float), P]),
             "dr_tuner_propose": (i32, [vp, i64, u64, i32, i32, P, ctypes.POINTER(i32)]),
             "dr_measure_peaks": (i32, [i32, ctypes.POINTER(Peaks)]),
+            "dr_debug_sieve_plan": (i64, [i64, i64, i32, i64, ctypes.POINTER(i64), i64]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -177,7 +178,7 @@ def exported_symbols() -> list:
         "dr_table_build_noalloc", "dr_autotune_batch",
         "dr_mlp_create", "dr_mlp_destroy", "dr_mlp_num_params", "dr_mlp_set_weights", "dr_mlp_get_weights",
         "dr_mlp_forward", "dr_mlp_grad", "dr_mlp_train", "dr_tuner_features", "dr_tuner_params", "dr_tuner_propose",
-        "dr_measure_peaks",
+        "dr_measure_peaks", "dr_debug_sieve_plan",
     ]
 
 
@@ -185,6 +186,16 @@ class Peaks(ctypes.Structure):
     """dr_peaks: measured ceilings, operations per second over the whole GPU."""
     _fields_ = [("smem_atomic_per_s", ctypes.c_double), ("smem_atomic_stride_per_s", ctypes.c_double),
                 ("imad_per_s", ctypes.c_double), ("dfma_per_s", ctypes.c_double)]
+
+
+def sieve_plan(u_total: int, u_dense: int, segment_log2: int, first_wave: int) -> list:
+    """The table build's sieve launches: (first segment, end segment, odd mode) in stream order."""
+    n = int(lib().dr_debug_sieve_plan(int(u_total), int(u_dense), int(segment_log2), int(first_wave), None, 0))
+    if n < 0:
+        _check(n)
+    buf = (ctypes.c_int64 * (3 * max(n, 1)))()
+    lib().dr_debug_sieve_plan(int(u_total), int(u_dense), int(segment_log2), int(first_wave), buf, n)
+    return [(buf[3 * i], buf[3 * i + 1], bool(buf[3 * i + 2])) for i in range(n)]
 
 
 def measure_peaks(device: int = 0) -> dict:

@@ -178,6 +178,13 @@ int dr_debug_piece(dr_ctx *ctx, const int32_t *piece, const uint64_t *q, int64_t
  * q >= 2^31 (outside their domains).  No counterpart in the reference. */
 int dr_debug_udiv32(dr_ctx *ctx, const uint64_t *y, const uint64_t *d, int64_t n, uint64_t *q);
 int dr_debug_piece32(dr_ctx *ctx, const int32_t *piece, const uint64_t *q, int64_t n, int64_t *out);
+/* Test support (no counterpart in the reference): the sieve launches a table build
+ * makes, as {first segment, end segment, odd mode} triples in stream order, for
+ * 2^segment_log2-value segments and a first wave of first_wave segments (one per
+ * full-mode CTA).  Writes at most cap triples; returns their number, or a negative
+ * DR_ERR_* code.  Needs no GPU. */
+int64_t dr_debug_sieve_plan(int64_t u_total, int64_t u_dense, int32_t segment_log2, int64_t first_wave,
+                            int64_t *out, int64_t cap);
 
 /* Measured throughput ceilings of the units this engine's kernels are bound by
  * (measurement support for bench.py; no counterpart in the reference).  Each is
