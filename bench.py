@@ -3,8 +3,8 @@
 
 One "step" is one complete M(10^16) through the engine: segmented Mobius sieve,
 dense + compressed Mertens tables, term planning, persistent S1/S2 kernel and
-the reduction -- nothing cached between steps (the 2.5 GB table is rebuilt
-every step, so every step's working set is far larger than the 126 MB L2).
+the reduction -- nothing cached between steps (the ~9 GB of tables and
+reciprocals are rebuilt every step, far larger than the 126 MB L2).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
@@ -12,6 +12,14 @@ N > 1 (torchrun, one process per GPU) runs N independent replicas: M(X) does
 not need a collective.  Rank 0 prints one JSON line.  The reference arm times
 the reference's own CPU engine (oracle/_ref, built from its sources) on this
 host's cores.
+
+Besides the contract's keys the line carries `phases_ms` (table, planning,
+sums), `roofline` (the S1/S2 phase against the HBM copy peak), `int_peaks`
+(shared-memory atomic, IMAD and DFMA ceilings measured on this GPU by
+dr_measure_peaks), `table_roofline` (the sieve's atomics per second against
+those ceilings and the table writes against HBM), `default_params` and
+`learned_tuner` (the same step with the reference's parameters and with the
+learned tuner's proposal) and `batched` (the 256-query batch).
 """
 from __future__ import annotations
 
