@@ -4,7 +4,10 @@
 //                    three table outputs of each segment: dense int16 prefix,
 //                    compressed bit planes + checkpoints, Mobius wheel bits
 //                    (mertens_dr.hpp:755-883 for the streamed builder,
-//                    :180-296 / :300-368 for the dense one)
+//                    :180-296 / :300-368 for the dense one); full mode sieves
+//                    every value, odd mode the odd values only and derives the
+//                    even ones from the planes of their halves
+//  sq_bucket_*       per-segment hit lists of the squares p^2 > S
 //  seg_scan_kernel   exclusive scan of per-segment Mobius sums
 //  fixup_kernel      global offsets into the dense prefix and checkpoints
 //                    (mertens_dr.hpp:884-900)
