@@ -206,7 +206,8 @@ def run_reference(args, world, rank):
 
 
 KNOWN = {10**k: m for k, m in [(9, -222), (10, -33722), (11, -87856), (12, 62366), (13, 599582), (14, -875575),
-                                    (15, -3216373), (16, -3195437), (17, -21830254)]}  # test_dr.cpp, test_cuda.cu, README
+                                    (15, -3216373), (16, -3195437), (17, -21830254), (18, -46758740)]}
+# test_dr.cpp, test_cuda.cu, README; 10^18 pinned by the reference engine built from its own sources
 
 
 def sieve_marks(u_total, u_dense, sm_count, S=1 << 17):
@@ -389,7 +390,7 @@ def run_engine(args, world, rank, local):
     alg = 2 * s0_.s1_ops + 0.5 * s0_.s2_ops
     achieved = alg / (sums / 1e3) / 1e9
     # DRAM traffic: ncu dram__bytes_read.sum + dram__bytes_write.sum of sums_kernel
-    # in a 1-pass capture of M(10^16) with these parameters (profiles/launches_m1e16.md):
+    # in a 1-pass capture of M(10^16) with these parameters:
     # 87.2 GB for 4.35e10 ops = 2.0 B per op, times this call's op count.
     traffic = 2.0 * (s0_.s1_ops + s0_.s2_ops)
     # Table build: shared-memory atomic marks issued by the sieve per second against the

@@ -272,6 +272,10 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
                 dr_stats* st) {
     int rc = check_table_limits(u_total, u_dense, mu_limit);
     if (rc) return rc;
+    // From here on the old table is gone or being overwritten (a buffer may be
+    // freed and regrown, or a launch fail partway): the table is valid again only
+    // once every launch of this build has been enqueued.
+    c->table_valid = false;
     const int S = pick_segment(tuning);
     const int block = (tuning && tuning->block_threads) ? tuning->block_threads : 1024;
     if (block < 128 || block > 1024 || (block & 31))
@@ -329,6 +333,7 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
         m.sqB_first = k;
         std::vector<uint4> items(kMaxSieveItems);
         m.n_items = build_sieve_items(pr.data(), (int)pr.size(), B, items.data(), kMaxSieveItems);
+        if (m.n_items < 0) return fail(DR_ERR_PARAMS, "sieve work items exceed %d for %d bytes per segment", kMaxSieveItems, B);
         int e = ensure(c, buf, (size_t)std::max(m.n_items, 1) * 16);
         if (e) return e;
         if (m.n_items) {
@@ -912,8 +917,20 @@ int dr_default_params(int64_t X, int policy, dr_params* out) {
         if (X <= 100000LL) ref_dense_params(X, out);
         else gpu_params(X, out);
         return DR_OK;
+    case DR_POLICY_REFERENCE_GPU: ref_gpu_params(X, 0, out); return DR_OK;
     }
     return fail(DR_ERR_ARG, "unknown policy %d", policy);
+}
+
+int dr_reference_gpu_params(int64_t X, int host_threads, dr_params* out) {
+    if (!out) return fail(DR_ERR_ARG, "out is NULL");
+    params_clear(out);
+    if (X < 1) {
+        out->cx = ref_choose_cx(X);
+        return DR_OK;
+    }
+    ref_gpu_params(X, host_threads, out);
+    return DR_OK;
 }
 
 uint64_t dr_table_bytes(int64_t u_total, int64_t u_dense, int64_t mu_limit) {
@@ -1014,6 +1031,7 @@ int dr_mertens_batch(dr_ctx* c, const int64_t* X, int64_t count, const dr_params
     if (count > 1) {
         for (auto& g : c->graphs) {
             if (!same_batch(g, X, P.data(), count, tune)) continue;
+            c->table_valid = false;  // the graph rebuilds the table in place
             CU(cudaGraphLaunch(g.exec, c->stream));
             c->table_valid = true;
             c->t_u_total = ut;

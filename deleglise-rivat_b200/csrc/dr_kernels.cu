@@ -601,13 +601,17 @@ int build_sieve_items(const uint32_t* primes, int n_primes, int S, uint4* out, i
         const uint32_t p = primes[i];
         if (p >= 13 && p < lim) {
             const uint32_t w = (32u - (uint32_t)__builtin_clz(p - 1)) | 1u;
-            for (uint32_t st = 0; st < (uint32_t)S; st += 1024u * p)
-                if (n < cap) out[n++] = make_uint4(p, st, w, (uint32_t)i);
+            for (uint32_t st = 0; st < (uint32_t)S; st += 1024u * p) {
+                if (n >= cap) return -1;  // an item would be dropped: its marks would be missing
+                out[n++] = make_uint4(p, st, w, (uint32_t)i);
+            }
         }
         if (p >= 5 && p * p < lim) {
             const uint32_t q = p * p;
-            for (uint32_t st = 0; st < (uint32_t)S; st += 1024u * q)
-                if (n < cap) out[n++] = make_uint4(q, st, 0x80u, (uint32_t)i | 0x80000000u);
+            for (uint32_t st = 0; st < (uint32_t)S; st += 1024u * q) {
+                if (n >= cap) return -1;
+                out[n++] = make_uint4(q, st, 0x80u, (uint32_t)i | 0x80000000u);
+            }
         }
     }
     return n;

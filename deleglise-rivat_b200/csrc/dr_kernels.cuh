@@ -114,7 +114,10 @@ void launch_sq_bucket_fill(const uint32_t* primes, int first, int n, i64 u_total
 // cut into pieces of at most 1024 hits (32 lanes x 32 strides), so that the
 // warps of a CTA get equal shares of the marking instead of one warp holding
 // p = 13.  Items are ordered by prime index: the items valid for the first n
-// primes are a prefix.  Returns the count written (<= cap).
+// primes are a prefix.  Returns the count written (<= cap), or -1 if the items
+// do not fit in cap (none is ever dropped silently: a missing item would leave
+// marks out and the Mobius values wrong).  For the sieved bytes per segment used
+// here (at most 2^17) there are fewer than 700 items.
 constexpr int kMaxSieveItems = 2048;
 int build_sieve_items(const uint32_t* primes, int n_primes, int S, uint4* out, int cap);
 // Number of leading items whose prime index is below n_primes.

@@ -16,7 +16,6 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <functional>
 #include <mutex>
 
 #include "../../include/dr_engine.h"
@@ -47,7 +46,7 @@ static_assert(kOffItems % 4 == 0, "uint4 items need 16-byte alignment");
 
 // The scratch.  In host code this name is only a host-side stand-in for the
 // symbol, never a device address: the device address comes from
-// cudaGetSymbolAddress() below, once per device.
+// cudaGetSymbolAddress() below, on every call, with the device current.
 static __device__ __align__(256) uint32_t g_table_scratch[kScratchWords];
 
 // Host-side constant inputs, filled once per process (static storage, no heap).
@@ -69,6 +68,7 @@ void fill_host_constants() {
         g_host_primes[g_host_prime_count++] = (uint32_t)p;
         for (int64_t m = p * p; m <= kNoAllocMaxRoot; m += p) composite[m] = 1;
     }
+    // a negative count means the items did not fit (set-up then fails)
     g_host_item_count = build_sieve_items(g_host_primes, g_host_prime_count, kNoAllocSeg, g_host_items, kMaxSieveItems);
     // periodic stencil, 4 copies shifted by 0..3 bytes; byte i describes n = i + 1
     auto stencil_byte = [](int i) -> uint32_t {
@@ -88,14 +88,52 @@ void fill_host_constants() {
         }
 }
 
+// Per-device set-up state.  `done` is set only after a set-up that succeeded, so
+// a failed set-up is retried by the next call.  `ctx_id` is the unique id of the
+// CUDA context the set-up ran in: a device reset (cudaDeviceReset, or any other
+// replacement of the primary context) reloads the module, which loses the
+// scratch's contents and may move it, so a call in another context runs the
+// set-up again.
 struct DeviceSetup {
-    std::once_flag once;
-    int status = DR_OK;
+    std::mutex mu;
+    bool done = false;
+    unsigned long long ctx_id = 0;
     uint32_t* scratch = nullptr;  // device address of g_table_scratch on this device
     int sieve_per_sm = 1;
     int sm_count = 1;
 };
 DeviceSetup g_dev[kMaxDevices];
+
+// Unique id of the current CUDA context (cuCtxGetId through the runtime's driver
+// entry points, so that the library needs no link against libcuda).
+typedef int (*CtxGetCurrentFn)(void**);
+typedef int (*CtxGetIdFn)(void*, unsigned long long*);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+std::once_flag g_entry_once;
+
+void load_entry_points() {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+        g_ctx_get_current = (CtxGetCurrentFn)f;
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+        g_ctx_get_id = (CtxGetIdFn)f;
+    cudaGetLastError();
+}
+
+// 0 where the id cannot be read (set-up then keys on the scratch address alone)
+unsigned long long current_ctx_id() {
+    std::call_once(g_entry_once, load_entry_points);
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (!g_ctx_get_current || !g_ctx_get_id || g_ctx_get_current(&ctx) != 0 || !ctx) return 0;
+    if (g_ctx_get_id(ctx, &id) != 0) return 0;
+    return id;
+}
 
 int noalloc_fail(int code, const char* msg, cudaError_t e = cudaSuccess) {
     char buf[256];
@@ -104,42 +142,38 @@ int noalloc_fail(int code, const char* msg, cudaError_t e = cudaSuccess) {
     return record_error(code, buf);
 }
 
-// Once per device, with that device current: resolve the scratch's device
-// address and fill its constant parts (stencil, primes).
-void setup_device(int device, DeviceSetup& d) {
+// With the device current and d.mu held: fill the scratch's constant parts
+// (stencil, primes, reciprocals, work items) at device address ptr.  Returns
+// DR_OK and marks the set-up done only when every step succeeded.
+int setup_device(int device, DeviceSetup& d, uint32_t* ptr, unsigned long long ctx_id) {
     std::call_once(g_host_once, fill_host_constants);
-    void* ptr = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&ptr, g_table_scratch);
-    if (e != cudaSuccess || !ptr) {
-        d.status = noalloc_fail(DR_ERR_CUDA, "cudaGetSymbolAddress(g_table_scratch) failed", e);
-        return;
-    }
-    d.scratch = (uint32_t*)ptr;
-    e = cudaMemcpy(d.scratch + kOffStencil, g_host_stencil, sizeof(g_host_stencil), cudaMemcpyHostToDevice);
+    d.done = false;
+    if (g_host_item_count < 0) return noalloc_fail(DR_ERR_ARG, "sieve work items exceed their fixed capacity");
+    cudaError_t e = cudaMemcpy(ptr + kOffStencil, g_host_stencil, sizeof(g_host_stencil), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
-        e = cudaMemcpy(d.scratch + kOffPrimes, g_host_primes, sizeof(uint32_t) * (size_t)g_host_prime_count,
+        e = cudaMemcpy(ptr + kOffPrimes, g_host_primes, sizeof(uint32_t) * (size_t)g_host_prime_count,
                        cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
-        e = cudaMemcpy(d.scratch + kOffPinv, g_host_pinv, sizeof(uint64_t) * (size_t)g_host_prime_count,
+        e = cudaMemcpy(ptr + kOffPinv, g_host_pinv, sizeof(uint64_t) * (size_t)g_host_prime_count,
                        cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
-        e = cudaMemcpy(d.scratch + kOffSqinv, g_host_sqinv, sizeof(uint64_t) * (size_t)g_host_prime_count,
+        e = cudaMemcpy(ptr + kOffSqinv, g_host_sqinv, sizeof(uint64_t) * (size_t)g_host_prime_count,
                        cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
-        e = cudaMemcpy(d.scratch + kOffItems, g_host_items, sizeof(uint4) * (size_t)g_host_item_count,
+        e = cudaMemcpy(ptr + kOffItems, g_host_items, sizeof(uint4) * (size_t)g_host_item_count,
                        cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) {
-        d.status = noalloc_fail(DR_ERR_CUDA, "filling the table scratch failed", e);
-        return;
-    }
+    if (e != cudaSuccess) return noalloc_fail(DR_ERR_CUDA, "filling the table scratch failed", e);
     e = cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, device);
-    if (e != cudaSuccess) {
-        d.status = noalloc_fail(DR_ERR_CUDA, "cudaDeviceGetAttribute failed", e);
-        return;
-    }
-    sieve_kernel_attrs(sieve_smem_bytes(kNoAllocSeg, false), false, 1024, &d.sieve_per_sm);
-    if (d.sieve_per_sm < 1) d.sieve_per_sm = 1;
-    d.status = DR_OK;
+    if (e != cudaSuccess) return noalloc_fail(DR_ERR_CUDA, "cudaDeviceGetAttribute failed", e);
+    int per_sm = 0;
+    sieve_kernel_attrs(sieve_smem_bytes(kNoAllocSeg, false), false, 1024, &per_sm);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return noalloc_fail(DR_ERR_CUDA, "sieve kernel attributes failed", e);
+    d.sieve_per_sm = std::max(per_sm, 1);
+    d.scratch = ptr;
+    d.ctx_id = ctx_id;
+    d.done = true;
+    return DR_OK;
 }
 
 int count_primes_upto(int64_t x) {  // over the static host list
@@ -183,8 +217,30 @@ extern "C" int dr_table_build_noalloc(int device, void* stream, int64_t u_total,
     if (prev != device && (e = cudaSetDevice(device)) != cudaSuccess)
         return noalloc_fail(DR_ERR_CUDA, "cudaSetDevice failed", e);
     DeviceSetup& d = g_dev[device];
-    std::call_once(d.once, setup_device, device, std::ref(d));
-    int rc = d.status;
+    int rc = DR_OK;
+    {
+        // The scratch's device address, looked up on every call (cheap): a device
+        // reset reloads the module, and the set-up reruns when the address or the
+        // context changed.  A set-up copies synchronously, which is illegal under
+        // stream capture, so it refuses a capturing stream before touching it.
+        std::lock_guard<std::mutex> lock(d.mu);
+        void* ptr = nullptr;
+        e = cudaGetSymbolAddress(&ptr, g_table_scratch);
+        if (e != cudaSuccess || !ptr) {
+            rc = noalloc_fail(DR_ERR_CUDA, "cudaGetSymbolAddress(g_table_scratch) failed", e);
+        } else {
+            const unsigned long long id = current_ctx_id();
+            if (!d.done || d.scratch != (uint32_t*)ptr || d.ctx_id != id) {
+                cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+                e = cudaStreamIsCapturing((cudaStream_t)stream, &cs);
+                if (e != cudaSuccess) rc = noalloc_fail(DR_ERR_CUDA, "cudaStreamIsCapturing failed", e);
+                else if (cs != cudaStreamCaptureStatusNone)
+                    rc = noalloc_fail(DR_ERR_ARG, "the first call on a device (or after a device reset) sets up the "
+                                                  "scratch synchronously and must not run under stream capture");
+                else rc = setup_device(device, d, (uint32_t*)ptr, id);
+            }
+        }
+    }
     if (rc == DR_OK) {
         cudaStream_t s = (cudaStream_t)stream;
         const int S = kNoAllocSeg;

@@ -4,13 +4,15 @@
 // engine's heuristics exactly (ecreeth/deleglise-rivat mertens_dr.hpp), so a
 // drop-in caller gets the same u, u_dense, cx and mu limit -- and therefore the
 // same intermediate S1/S2 checksums -- as the reference for the same X and
-// environment.  DR_POLICY_GPU is this engine's own default for B200.
+// environment.  DR_POLICY_REFERENCE_GPU restates the reference GPU engine's
+// choice (mertens_cuda.cuh).  DR_POLICY_GPU is this engine's own default for B200.
 #pragma once
 
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
+#include <thread>
 
 #include "../../include/dr_engine.h"
 
@@ -126,6 +128,55 @@ inline void ref_compressed_params(int64_t X, dr_params* p) {
     p->u_dense = u_dense;
     p->cx = cx;
     p->mu_limit = std::min(u_total, mu_limit);
+}
+
+// The thread count an OpenMP program uses by default (omp_get_max_threads() with
+// no other setting): the first entry of OMP_NUM_THREADS if set, else the number of
+// hardware threads.
+inline int default_host_threads() {
+    if (const char* e = std::getenv("OMP_NUM_THREADS")) {
+        const int v = std::atoi(e);
+        if (v > 0) return v;
+    }
+    const unsigned h = std::thread::hardware_concurrency();
+    return h ? (int)h : 1;
+}
+
+// The reference GPU engine's parameters (mertens_cuda.cuh): u from
+// choose_gpu_sieve_limit (:421-436) -- fx 1.10 / 1.45 / 2.20 at X below 10^15 /
+// from 10^15 / from 10^16, at least 3 sqrt(X), capped at 6e8 for 1 or 2 host
+// threads and 1.4e9 otherwise -- one dense table over [0, u] (SieveTable, :465),
+// cx from choose_cx (:473), mu limit min(u, max(N, cx sqrt X) + 65536) (:492).
+// At X <= 5e7 that engine calls the CPU engine (:458-460), whose dense parameters
+// are returned instead.  threads <= 0 stands for the host's default thread count.
+inline int64_t ref_gpu_sieve_limit(int64_t X, int threads) {
+    if (X <= 50000000LL) return X;
+    const double loglogX = std::log(std::max(2.0, std::log((double)X)));
+    double fx = 1.10;
+    if (X >= 1000000000000000LL) fx = 1.45;
+    if (X >= 10000000000000000LL) fx = 2.20;
+    int64_t u = (int64_t)(fx * std::pow((double)X / loglogX, 2.0 / 3.0));
+    const int64_t S = isqrt_i64(X);
+    if (u < 3 * S) u = 3 * S;
+    if (threads <= 0) threads = default_host_threads();
+    const int64_t cap = (threads > 0 && threads <= 2) ? 600000000LL : 1400000000LL;
+    return std::min(u, cap);
+}
+
+inline void ref_gpu_params(int64_t X, int threads, dr_params* p) {
+    if (X <= 50000000LL) {
+        ref_dense_params(X, p);
+        return;
+    }
+    params_clear(p);
+    const int64_t u = ref_gpu_sieve_limit(X, threads);
+    const double cx = ref_choose_cx(X);
+    const int64_t N = X / u;
+    const int64_t A = (int64_t)(cx * std::sqrt((double)X));
+    p->u_total = u;
+    p->u_dense = u;
+    p->cx = cx;
+    p->mu_limit = std::min<int64_t>(u, std::max(N, A) + 65536);
 }
 
 // B200 policy (DR_POLICY_GPU), fitted to sweeps of measured device times over

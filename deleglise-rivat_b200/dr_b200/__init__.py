@@ -33,6 +33,7 @@ POLICY_REFERENCE = 0
 POLICY_DENSE = 1
 POLICY_COMPRESSED = 2
 POLICY_GPU = 3
+POLICY_REFERENCE_GPU = 4
 
 
 class DRError(RuntimeError):
@@ -124,6 +125,7 @@ def lib():
             "dr_ctx_set_hbm_budget": (i32, [vp, u64]),
             "dr_device_info": (i32, [i32, ctypes.POINTER(i32), ctypes.POINTER(u64)]),
             "dr_default_params": (i32, [i64, i32, P]),
+            "dr_reference_gpu_params": (i32, [i64, i32, P]),
             "dr_check_params": (i32, [i64, P, u64]),
             "dr_table_bytes": (u64, [i64, i64, i64]),
             "dr_query_bytes": (u64, [i64, P]),
@@ -172,7 +174,7 @@ def exported_symbols() -> list:
     lib()
     return [
         "dr_ctx_create", "dr_ctx_destroy", "dr_last_error", "dr_ctx_set_hbm_budget", "dr_device_info",
-        "dr_default_params", "dr_check_params", "dr_table_bytes", "dr_query_bytes", "dr_mertens", "dr_mertens_batch",
+        "dr_default_params", "dr_reference_gpu_params", "dr_check_params", "dr_table_bytes", "dr_query_bytes", "dr_mertens", "dr_mertens_batch",
         "dr_batch_checksums", "dr_table_build", "dr_table_read", "dr_table_read_wheel", "dr_table_checksums",
         "dr_debug_udiv", "dr_debug_udiv_rcp", "dr_debug_udiv32", "dr_debug_piece", "dr_debug_piece32",
         "dr_table_build_noalloc", "dr_autotune_batch",
@@ -214,6 +216,13 @@ def default_params(X: int, policy: int = POLICY_REFERENCE) -> Params:
     """Reference parameter policy (choose_cx / choose_sieve_limit / choose_compressed_limit)."""
     p = Params()
     _check(lib().dr_default_params(int(X), int(policy), ctypes.byref(p)))
+    return p
+
+
+def reference_gpu_params(X: int, host_threads: int = 0) -> Params:
+    """The reference GPU engine's parameters (choose_gpu_sieve_limit, mertens_cuda.cuh:421)."""
+    p = Params()
+    _check(lib().dr_reference_gpu_params(int(X), int(host_threads), ctypes.byref(p)))
     return p
 
 

@@ -51,6 +51,8 @@ extern "C" {
 #define DR_POLICY_DENSE 1     /* reference dense path (MERTENS_USE_CHMT=0)  */
 #define DR_POLICY_COMPRESSED 2 /* reference streamed path (compute_compressed) */
 #define DR_POLICY_GPU 3       /* B200 defaults: larger u, compressed tier   */
+#define DR_POLICY_REFERENCE_GPU 4 /* the reference GPU engine's choice, default
+                                     host thread count (dr_reference_gpu_params) */
 
 typedef struct dr_ctx dr_ctx;
 
@@ -95,6 +97,13 @@ int dr_device_info(int device, int *sm_count, uint64_t *hbm_bytes);
 
 /* Parameters ------------------------------------------------------------- */
 int dr_default_params(int64_t X, int policy, dr_params *out);
+/* The parameters the reference GPU engine picks for X (mertens_cuda.cuh:421-436
+ * choose_gpu_sieve_limit, :473 cx, :492 mu limit): one dense table of u values,
+ * u capped at 6e8 for host_threads in {1, 2} and 1.4e9 otherwise (host_threads
+ * <= 0: OMP_NUM_THREADS, else the hardware thread count, as omp_get_max_threads()
+ * would give); at X <= 5e7 the reference CPU engine's dense parameters (that
+ * engine hands such X to compute_mertens, :458-460). */
+int dr_reference_gpu_params(int64_t X, int host_threads, dr_params *out);
 /* Endpoint-coverage and budget check (0 = usable). */
 int dr_check_params(int64_t X, const dr_params *p, uint64_t hbm_budget);
 /* Device bytes a table with these limits needs. */
@@ -226,7 +235,10 @@ int dr_measure_peaks(int device, dr_peaks *out);
  * waiting: the table is ready when the stream is.  The first call on a device
  * sets up the scratch for that device (it looks up the array's device address
  * and copies the primes and the stencil into it, synchronously); make that
- * first call before any stream capture.  All calls share the one scratch
+ * first call before any stream capture (on a capturing stream it returns
+ * DR_ERR_ARG and leaves the stream untouched).  A set-up that failed is retried
+ * by the next call, and a call in a new CUDA context of the device (after
+ * cudaDeviceReset) sets up again, synchronously.  All calls share the one scratch
  * array, which keeps the last call's contents, so calls whose work overlaps on
  * the GPU (other streams, other threads) race on it: serialise them. */
 #define DR_NOALLOC_MAX_U 8589934592LL

@@ -28,12 +28,24 @@ public:
         double total_time = 0.0;       // wall time of the call (seconds)
     };
 
+    // choose_gpu_sieve_limit :421-436: the reference GPU engine's u for X and its
+    // host thread count (it caps u lower for 1 or 2 threads)
+    static inline int64 choose_gpu_sieve_limit(int64 X, int threads) {
+        dr_params p;
+        mertens_dr::b200::check(dr_reference_gpu_params(X, threads > 0 ? threads : 0, &p));
+        return X <= 50000000LL ? X : (int64)p.u_total;
+    }
+
+    // The parameters are the reference GPU engine's for (X, host_threads):
+    // dr_reference_gpu_params restates them, so M(X) and the intermediate sums are
+    // those of the same decomposition.
     static int64 compute_mertens(int64 X, int host_threads = 0, TimingStats* stats = nullptr) {
-        (void)host_threads;
         if (X < 1) return 0;
         dr_stats st;
+        dr_params p;
         int64_t out = 0;
-        mertens_dr::b200::check(dr_mertens(mertens_dr::b200::context(), X, nullptr, &out, &st));
+        mertens_dr::b200::check(dr_reference_gpu_params(X, host_threads, &p));
+        mertens_dr::b200::check(dr_mertens(mertens_dr::b200::context(), X, &p, &out, &st));
         if (stats) {
             stats->host_sieve_time = st.table_ms / 1e3;
             stats->h2d_copy_time = st.h2d_ms / 1e3;

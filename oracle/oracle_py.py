@@ -138,6 +138,32 @@ class Oracle:
                                           mu.ctypes.data_as(ctypes.POINTER(ctypes.c_int8))))
 
 
+REF_GPU_PARAMS_SO = os.path.join(HERE, "_ref", "libdr_ref_gpu_params.so")
+
+
+class ReferenceGpuParams:
+    """The reference GPU engine's parameter heuristic, compiled from mertens_cuda.cuh
+    (choose_gpu_sieve_limit :421-436, cx :473, mu limit :492)."""
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(REF_GPU_PARAMS_SO)
+
+    def __init__(self):
+        L = ctypes.CDLL(REF_GPU_PARAMS_SO)
+        L.ref_gpu_sieve_limit.restype = i64
+        L.ref_gpu_sieve_limit.argtypes = [i64, c_int]
+        L.ref_gpu_cx.restype = c_double
+        L.ref_gpu_cx.argtypes = [i64]
+        L.ref_gpu_mu_limit.restype = i64
+        L.ref_gpu_mu_limit.argtypes = [i64, i64]
+        self.L = L
+
+    def params(self, X: int, threads: int):
+        u = int(self.L.ref_gpu_sieve_limit(int(X), int(threads)))
+        return u, float(self.L.ref_gpu_cx(int(X))), int(self.L.ref_gpu_mu_limit(int(X), u))
+
+
 class Reference:
     """The reference engine built from its own sources (oracle/_ref)."""
 

@@ -92,3 +92,52 @@ def test_no_gpu_fails_loudly():
         pass
     with pytest.raises(dr_b200.DRError):
         dr_b200.Engine(0)
+
+
+@pytest.mark.parametrize("threads", [1, 2, 3, 16, 0])
+def test_reference_gpu_policy_matches_reference_build(monkeypatch, threads):
+    """dr_reference_gpu_params against choose_gpu_sieve_limit / cx / mu limit of the
+    reference GPU engine compiled from its own header (oracle/_ref)."""
+    from oracle_py import ReferenceGpuParams
+
+    if not ReferenceGpuParams.available():
+        pytest.skip("reference build absent")
+    for k in ("MERTENS_CX", "OMP_NUM_THREADS"):
+        monkeypatch.delenv(k, raising=False)
+    ref = ReferenceGpuParams()
+    # threads 0: the engine's default thread count, omp_get_max_threads() = the host's cores
+    rt = threads if threads > 0 else (os.cpu_count() or 1)
+    for X in [5 * 10**7 + 1, 10**8, 10**9, 10**10, 10**11, 10**12, 10**13, 10**14, 10**15 - 1, 10**15, 10**16 - 1,
+              10**16, 10**17, 10**18]:
+        p = dr_b200.reference_gpu_params(X, threads)
+        u, cx, ml = ref.params(X, rt)
+        assert (p.u_total, p.u_dense, p.cx, p.mu_limit) == (u, u, cx, ml), (X, threads)
+        # where N = X/u exceeds the table (10^18 with u capped at 6e8 or 1.4e9) the
+        # reference's term loop would read mu past its table; the coverage check refuses
+        ok = X // u <= ml and int(cx * X ** 0.5) <= ml
+        assert dr_b200.check_params(X, p) == (0 if ok else dr_b200.DR_ERR_PARAMS), (X, threads)
+    # the policy constant uses the default thread count
+    q = dr_b200.default_params(10**15, dr_b200.POLICY_REFERENCE_GPU)
+    r = dr_b200.reference_gpu_params(10**15, 0)
+    assert (q.u_total, q.cx, q.mu_limit) == (r.u_total, r.cx, r.mu_limit)
+    # X <= 5e7: that engine hands X to the CPU engine's dense path
+    small = dr_b200.reference_gpu_params(10**7, threads)
+    dense = dr_b200.default_params(10**7, dr_b200.POLICY_DENSE)
+    assert (small.u_total, small.cx, small.mu_limit) == (dense.u_total, dense.cx, dense.mu_limit)
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch():
+    """dr_table_build_noalloc checks its arguments before any CUDA call: u_total
+    above DR_NOALLOC_MAX_U = 2^33 (the fixed scratch's limit) is DR_ERR_ARG."""
+    import ctypes
+
+    f = dr_b200.lib().dr_table_build_noalloc
+    buf = ctypes.c_void_p(1 << 20)  # never dereferenced: the call fails first
+    for ut, ud, ml in [((1 << 33) + 1, 0, 1000), (1 << 40, 1 << 20, 1000), (0, 0, 0), (100, 200, 10), (100, 10, 101)]:
+        rc = f(0, None, ut, ud, ml, buf, buf, buf, buf)
+        assert rc == dr_b200.DR_ERR_ARG, (ut, ud, ml, rc)
+    assert b"2^33" in dr_b200.lib().dr_last_error() or b"u_" in dr_b200.lib().dr_last_error()
+    rc = f(0, None, (1 << 33) + 1, 0, 1000, buf, buf, buf, buf)
+    assert b"DR_NOALLOC_MAX_U" in dr_b200.lib().dr_last_error()
+    rc = f(-1, None, 1000, 0, 10, buf, buf, buf, buf)
+    assert rc == dr_b200.DR_ERR_ARG

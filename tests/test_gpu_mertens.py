@@ -100,13 +100,51 @@ def test_gpu_policy_known_answers(engine):
         assert engine.mertens(c["X"], p).M == c["M"], c
 
 
-def test_m1e18(engine):
+def _m1e18(engine, p):
     # pinned only by the reference engine's own run (tests/golden/m1e18.json)
     g = load_golden("m1e18.json")
-    p = dr_b200.default_params(g["X"], dr_b200.POLICY_GPU)
+    assert dr_b200.check_params(g["X"], p) == 0
     r = engine.mertens(g["X"], p)
-    assert r.M == g["M"]
+    assert r.M == g["M"], p
     assert (r.stats.C - r.stats.S1 - r.stats.S2) % (1 << 64) == g["M"] % (1 << 64)
+    return r
+
+
+def test_m1e18(engine):
+    # the B200 policy: u = 2.5e11 values, 94 GB of device data
+    _m1e18(engine, dr_b200.default_params(10**18, dr_b200.POLICY_GPU))
+
+
+def test_m1e18_reference_default_params(engine):
+    """M(10^18) with the reference's own default parameters (compute_compressed,
+    mertens_dr.hpp:1442-1461): u = 8e9 (its cap), u_dense = 1,350,001,152, cx = 1.35."""
+    p = dr_b200.default_params(10**18, dr_b200.POLICY_REFERENCE)
+    assert (p.u_total, p.u_dense, p.cx) == (8000000000, 1350001152, 1.35)
+    r = _m1e18(engine, p)
+    assert r.stats.terms > 0
+
+
+def test_m1e18_learned_tuner_params(engine):
+    """M(10^18) with the learned tuner's proposal (the committed weights; X = 10^18
+    lies beyond the training domain, so the proposal is carried along the X^(2/3)
+    law from its edge) -- no fallback to the reference heuristic."""
+    import json
+    import os
+
+    import numpy as np
+
+    path = os.path.join(os.path.dirname(dr_b200.__file__), "tuner_weights.json")
+    with open(path) as f:
+        w = np.array(json.load(f)["weights"], dtype=np.float32)
+    mlp = dr_b200.MLP(engine)
+    try:
+        mlp.set_weights(w)
+        _, hbm = dr_b200.device_info(0)
+        p, fb = mlp.propose(10**18, int(hbm * 0.9), 148, 1)
+    finally:
+        mlp.close()
+    assert not fb
+    _m1e18(engine, p)
 
 
 def test_windowed_s1_matches_direct(engine):

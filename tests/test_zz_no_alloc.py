@@ -98,3 +98,61 @@ def test_noalloc_table_matches_allocating_build():
             M_ref, _ = eng.table_read(ut - 199999, 200000)
             assert np.array_equal(_compressed_M(planes_h, ckpt_h, ud, ut)[-200000:], M_ref)
     eng.close()
+
+
+def test_noalloc_at_its_size_limit():
+    """u_total = DR_NOALLOC_MAX_U = 2^33 with a small dense tier (about 2.7 GB of
+    caller buffers): 65,537 segments of scratch sums, all 8,952 sieving primes up to
+    92,681 and squares p^2 above 2^32 -- the upper bounds of the fixed scratch.  The
+    table checksums and sampled M(n) windows equal dr_table_build's at the same limits."""
+    import torch
+
+    f = dr_b200.lib().dr_table_build_noalloc
+    ut, ud, ml = 1 << 33, 1 << 20, 3000000
+    W = (ut - ud + 63) // 64
+    G = ml // 192 + 2
+    dM = torch.empty(ud, dtype=torch.int16, device="cuda")
+    planes = torch.empty(2 * W, dtype=torch.int64, device="cuda")
+    ckpt = torch.empty(W, dtype=torch.int32, device="cuda")
+    wheel = torch.full((4 * G,), -1, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    rc = f(0, ctypes.c_void_p(stream.cuda_stream), ut, ud, ml, ctypes.c_void_p(dM.data_ptr()),
+           ctypes.c_void_p(planes.data_ptr()), ctypes.c_void_p(ckpt.data_ptr()), ctypes.c_void_p(wheel.data_ptr()))
+    assert rc == 0, dr_b200.lib().dr_last_error().decode()
+    torch.cuda.synchronize()
+    # the checksums of dr_table_sums, computed on the device (int64 arithmetic wraps mod 2^64)
+    mask = (1 << 64) - 1
+    n = torch.arange(1, ud + 1, dtype=torch.int64, device="cuda")
+    d64 = dM.to(torch.int64)
+    k = torch.arange(W, dtype=torch.int64, device="cuda") * 2 + 1
+    pw = planes.view(-1, 2)
+    mine = (int(d64.sum()) & mask, int((d64 * (2 * n + 1)).sum()) & mask, int((pw[:, 0] * k).sum()) & mask,
+            int((pw[:, 1] * k).sum()) & mask, int((ckpt.to(torch.int64) * k).sum()) & mask)
+    del n, d64, k, pw
+    dM_h = dM.cpu().numpy()
+    tail = 200000
+    planes_t = planes[-2 * ((tail + 63) // 64 + 1):].cpu().numpy()
+    ckpt_t = ckpt[-((tail + 63) // 64 + 1):].cpu().numpy()
+    wheel_h = wheel.cpu().numpy()
+    del dM, planes, ckpt, wheel
+    torch.cuda.empty_cache()
+
+    eng = dr_b200.Engine(0)
+    try:
+        eng.table_build(ut, ud, ml)
+        ref = eng.table_checksums()
+        assert mine == (ref[0], ref[1], ref[3], ref[4], ref[5])
+        M_ref, _ = eng.table_read(1, 100000)
+        assert np.array_equal(dM_h[:100000].astype(np.int32), M_ref)
+        # the last values of the compressed tier: the planes and checkpoints of the tail words
+        wt = len(ckpt_t)
+        first_word = W - wt
+        off0 = first_word * 64
+        M_tail = _compressed_M(planes_t, ckpt_t, ud + off0, ut)
+        M_ref, _ = eng.table_read(ut - tail + 1, tail)
+        assert np.array_equal(M_tail[-tail:], M_ref)
+        nn = np.arange(1, ml + 1, dtype=np.int64)
+        cop = (nn % 2 == 1) & (nn % 3 != 0)
+        assert np.array_equal(_wheel_mu(wheel_h, nn[cop]), eng.table_read_wheel(1, ml)[cop])
+    finally:
+        eng.close()
