@@ -101,6 +101,11 @@ int64_t dro_mertens(int64_t X, int threads);
 /* Direct Mobius prefix for small X (independent check; O(X) memory). */
 int64_t dro_mertens_direct(int64_t X);
 
+/* Independent cross-check (dirichlet_dp.c): M(x) from sum_{d<=x} M(x/d) = 1 over
+ * a sieved Mobius prefix up to x^(2/3); no part of the Deleglise-Rivat path.
+ * INT64_MIN if memory runs out. */
+int64_t dro_mertens_dirichlet(int64_t x);
+
 #ifdef __cplusplus
 }
 #endif

@@ -69,6 +69,7 @@ class Oracle:
             "dro_mertens_params": (c_int, [ctypes.POINTER(OParams), c_int, ctypes.POINTER(OResult)]),
             "dro_mertens": (i64, [i64, c_int]),
             "dro_mertens_direct": (i64, [i64]),
+            "dro_mertens_dirichlet": (i64, [i64]),
         }
         for n, (r, a) in sig.items():
             f = getattr(L, n)
@@ -86,6 +87,10 @@ class Oracle:
 
     def mertens_direct(self, X: int) -> int:
         return int(self.L.dro_mertens_direct(int(X)))
+
+    def mertens_dirichlet(self, X: int) -> int:
+        """The independent second method (dirichlet_dp.c), not Deleglise-Rivat."""
+        return int(self.L.dro_mertens_dirichlet(int(X)))
 
     def run(self, X: int, u_total: int, u_dense: int, cx: float, mu_limit: int, threads: int = 0) -> dict:
         p = OParams(int(X), int(u_total), int(u_dense), float(cx), int(mu_limit))

@@ -135,3 +135,36 @@ def test_oracle_finalize_vs_reference(oracle, reference):
         mine = np.array([oracle.L.dro_finalize_byte(int(v), first + i) & 0xFF for i, v in enumerate(vals)],
                         dtype=np.uint8)
         assert np.array_equal(ref, mine), first
+
+
+# The reference's own cross-validation points (test_dr.cpp:74-76) and its known answers
+CROSS = [54321, 987654, 12345678, 987654321, 5000000000, 123456789012, 1000000000000]
+_DIRICHLET = {}
+
+
+def _dirichlet(oracle, x):
+    if x not in _DIRICHLET:
+        _DIRICHLET[x] = oracle.mertens_dirichlet(x)
+    return _DIRICHLET[x]
+
+
+def test_independent_method_vs_known_answers(oracle):
+    """The second method (sum_{d<=x} M(x/d) = 1, dirichlet_dp.c) reproduces the
+    reference's published known answers and equals the direct sieve on small x."""
+    for c in load_golden("kat.json")["cases"]:
+        if c["X"] <= 10**12:
+            assert _dirichlet(oracle, c["X"]) == c["M"], c
+    for x in list(range(0, 300)) + [999, 1000, 1001, 65536, 99975680]:
+        assert oracle.mertens_dirichlet(x) == oracle.mertens_direct(x), x
+
+
+def test_independent_method_vs_deleglise_rivat(oracle):
+    """Cross-validation as in test_dr.cpp:69-89: the Deleglise-Rivat restatement and
+    the independent method agree at the reference's cross-check points."""
+    for x in CROSS:
+        assert oracle.mertens(x) == _dirichlet(oracle, x), x
+
+
+def test_independent_method_vs_reference(reference, oracle):
+    for x in CROSS:
+        assert reference.compute_mertens(x) == _dirichlet(oracle, x), x
