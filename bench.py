@@ -233,6 +233,69 @@ def sieve_marks(u_total, u_dense, sm_count, S=1 << 17):
     return int(full.sum() + odd.sum())
 
 
+# Warp instructions per unit of work, from ncu smsp__inst_executed.sum of one launch
+# divided by that launch's work (the captures run at M(10^15) and on the M(10^15)
+# table; the mix per op is set by the per-lookup / per-position / per-value code):
+#   sums_kernel: per S1 lookup and per S2 wheel position (split by the two
+#     timing-only captures that keep one of the two parts, whose sum matches the
+#     whole kernel's count within 2%);
+#   sieve_kernel (odd mode): per table value.
+SUMS_INST_PER_S1 = 0.68
+SUMS_INST_PER_S2 = 1.57
+SIEVE_INST_PER_VALUE = 1.0
+# DRAM bytes per op of sums_kernel (dram__bytes_read.sum + dram__bytes_write.sum of
+# one launch over its S1 lookups + S2 positions) at M(10^15) ...
+SUMS_DRAM_PER_OP = 1.05
+
+
+def sums_roofline(st, sums_ms, peak, peak_kind, issue_peak, f_mhz):
+    """S1/S2 phase (sums_kernel) against HBM on the algorithmic bytes -- 2 B per
+    dense-tier S1 lookup, 20 B per compressed-tier lookup (16 B plane pair + 4 B
+    checkpoint), 1 B of Mobius value per S2 candidate j (two per wheel position) --
+    and against its binding unit, instruction issue."""
+    t = sums_ms / 1e3
+    dense = st.s1_ops - st.s1_comp_ops
+    alg = 2.0 * dense + 20.0 * st.s1_comp_ops + 2.0 * st.s2_ops
+    inst = SUMS_INST_PER_S1 * st.s1_ops + SUMS_INST_PER_S2 * st.s2_ops
+    return {
+        "bound": "hbm", "kernel": "sums_kernel (S1/S2 phase)", "achieved": alg / t / 1e9, "peak": peak,
+        "unit": "GB/s", "frac": alg / t / 1e9 / peak, "peak_kind": peak_kind,
+        "traffic": SUMS_DRAM_PER_OP * (st.s1_ops + st.s2_ops),
+        "traffic_basis": "ncu DRAM bytes per op of one sums_kernel launch at M(10^15), times this call's op count",
+        "alg_bytes": alg,
+        "ops": {"s1_lookups": st.s1_ops, "s1_compressed": st.s1_comp_ops, "s2_positions": st.s2_ops},
+        "ops_per_s": (st.s1_ops + st.s2_ops) / t,
+        "issue": {"bound": "instruction issue (binding)", "warp_inst": inst, "achieved": inst / t,
+                  "peak": issue_peak, "unit": "warp instructions/s", "frac": inst / t / issue_peak,
+                  "basis": f"{SUMS_INST_PER_S1} warp instructions per S1 lookup + {SUMS_INST_PER_S2} per S2 "
+                           f"position (ncu at M(10^15)); peak = SMs x 4 x {f_mhz:.0f} MHz"},
+    }
+
+
+def sieve_roofline(p, tab_ms, peak, peaks_int, issue_peak, sms):
+    """Table phase against its binding unit (instruction issue), the shared-memory
+    atomics it issues, and HBM on the table's algorithmic bytes."""
+    t = tab_ms / 1e3
+    seg = 1 << (p.segment_log2 or 18)
+    marks = sieve_marks(p.u_total, p.u_dense, sms, seg)
+    tbytes = 2 * p.u_dense + 0.3125 * (p.u_total - p.u_dense) + p.mu_limit / 4
+    inst = SIEVE_INST_PER_VALUE * p.u_total
+    return {
+        "kernel": "sieve_kernel (whole table phase: sieve, bucket, scan and fixup launches)",
+        "bound": "instruction issue", "achieved": inst / t, "peak": issue_peak, "unit": "warp instructions/s",
+        "frac": inst / t / issue_peak,
+        "basis": f"{SIEVE_INST_PER_VALUE} warp instructions per table value (ncu, odd-mode sieve on the "
+                 f"M(10^15) table); peak = SMs x 4 x SM clock",
+        "atomics": {"marks": marks, "achieved": marks / t, "peak": peaks_int["smem_atomic_per_s"],
+                    "peak_sieve_pattern": peaks_int["smem_atomic_stride_per_s"], "unit": "atomics/s",
+                    "frac": marks / t / peaks_int["smem_atomic_per_s"],
+                    "frac_of_sieve_pattern": marks / t / peaks_int["smem_atomic_stride_per_s"],
+                    "peak_kind": "measured on this GPU by dr_measure_peaks (synthetic kernels)"},
+        "hbm": {"bytes": tbytes, "achieved": tbytes / t / 1e9, "peak": peak, "unit": "GB/s",
+                "frac": tbytes / t / 1e9 / peak},
+    }
+
+
 def run_table_only(args, eng, stream):
     """Time the table build alone (sieve + prefix + compressed tier): --table u_total[,u_dense[,mu_limit]]."""
     import torch
@@ -382,33 +445,14 @@ def run_engine(args, world, rank, local):
     peak, peak_kind = load_peaks()
     s0_ = stats[0]
     phases = {"table_ms": tab, "plan_ms": plan, "sums_ms": sums}
-    # dominant phase: S1/S2 (sums_kernel; with the windowed S1 switched on, s1win_kernel
-    # as well), timed by the engine's CUDA events.  Algorithmic bytes: the Mertens value of every S1
-    # lookup (2 B, int16 dense tier) and the Mobius bits of every S2 wheel position
-    # (0.5 B); reciprocal tables are a cache of this implementation and are not
-    # counted.  ops_per_s is the figure the kernels are optimised on.
-    alg = 2 * s0_.s1_ops + 0.5 * s0_.s2_ops
-    achieved = alg / (sums / 1e3) / 1e9
-    # DRAM traffic: ncu dram__bytes_read.sum + dram__bytes_write.sum of sums_kernel
-    # in a 1-pass capture of M(10^16) with these parameters:
-    # 87.2 GB for 4.35e10 ops = 2.0 B per op, times this call's op count.
-    traffic = 2.0 * (s0_.s1_ops + s0_.s2_ops)
-    # Table build: shared-memory atomic marks issued by the sieve per second against the
-    # measured ceiling, and the table's HBM writes against the copy peak.
-    marks = sieve_marks(tuned.u_total, tuned.u_dense, torch.cuda.get_device_properties(local).multi_processor_count,
-                        1 << (tuned.segment_log2 or 17))
-    tbytes = 2 * tuned.u_dense + 0.3125 * (tuned.u_total - tuned.u_dense) + tuned.mu_limit / 4
-    table_roofline = {
-        "kernel": "sieve_kernel (whole table phase: sieve, bucket, scan and fixup launches)",
-        "bound": "shared-memory atomics / integer issue", "marks": marks,
-        "achieved": marks / (tab / 1e3), "peak": peaks_int["smem_atomic_per_s"],
-        "peak_sieve_pattern": peaks_int["smem_atomic_stride_per_s"], "unit": "atomics/s",
-        "frac": marks / (tab / 1e3) / peaks_int["smem_atomic_per_s"],
-        "frac_of_sieve_pattern": marks / (tab / 1e3) / peaks_int["smem_atomic_stride_per_s"],
-        "hbm": {"bytes": tbytes, "achieved": tbytes / (tab / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-                "frac": tbytes / (tab / 1e3) / 1e9 / peak},
-        "peak_kind": "measured on this GPU by dr_measure_peaks (synthetic kernels)",
-    }
+    clk = clocks.summary()
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    # issue ceiling: 4 warp instructions per SM and clock at the median SM clock
+    # sampled during the timed region (the maximum clock where none was sampled)
+    f_mhz = clk["sm_mhz"] or clk["sm_max_mhz"] or 1965.0
+    issue_peak = sms * 4 * f_mhz * 1e6
+    roofline = sums_roofline(s0_, sums, peak, peak_kind, issue_peak, f_mhz)
+    table_roofline = sieve_roofline(tuned, tab, peak, peaks_int, issue_peak, sms)
     line = {
         "metric": "sec per M(10^16)" if X == X_HEADLINE else f"sec per M({X})", "value": value, "unit": "s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_per * 1e3,
@@ -425,15 +469,10 @@ def run_engine(args, world, rank, local):
         "gpu_launches": launches,
         "e2e": {"value": host_per / world, "unit": "s", "h2d_bytes_per_step": int(s0_.h2d_bytes),
                 "d2h_bytes_per_step": int(s0_.d2h_bytes)},
-        "roofline": {"bound": "hbm", "kernel": "sums_kernel (S1/S2 phase)", "achieved": achieved,
-                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                     "traffic_basis": "ncu DRAM bytes per op of sums_kernel at M(10^16), times the op count",
-                     "ops": {"s1_lookups": s0_.s1_ops, "s2_positions": s0_.s2_ops},
-                     "note": "sums_kernel: far S1 lookups cost a random DRAM sector each (1.3 TB/s of 32 B sectors), near ones and the S2 wheel stream hit L2; issue 57% active; ops_per_s = S1 lookups + S2 positions per second",
-                     "ops_per_s": (s0_.s1_ops + s0_.s2_ops) / (sums / 1e3)},
+        "roofline": roofline,
         "table_roofline": table_roofline,
         "int_peaks": peaks_int,
-        "clocks": clocks.summary(),
+        "clocks": clk,
         "batched": batch,
     }
     if rank == 0 and not args.no_cpu_baseline:

@@ -598,7 +598,7 @@ int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq,
     const int64_t invw_count = c->t_mu_limit / 6 + 1;  // every S2 j <= A <= mu_limit
     if ((rc = ensure(c, c->queries, (size_t)nq * sizeof(QueryDev)))) return rc;
     if ((rc = ensure(c, c->acc, (size_t)nq * 3 * 8))) return rc;
-    if ((rc = ensure(c, c->counts, (size_t)nq * 4 * 8))) return rc;
+    if ((rc = ensure(c, c->counts, (size_t)nq * kCountsPerQuery * 8))) return rc;
     if ((rc = ensure(c, c->ops, (size_t)std::max<u64>(slots, 1) * 8))) return rc;
     if ((rc = ensure(c, c->prefix, (size_t)(slots + 1) * 8))) return rc;
     if ((rc = ensure(c, c->scan_tmp, scan_u64_tmp_elems(slots) * 8))) return rc;
@@ -609,7 +609,7 @@ int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq,
     }
     if ((rc = ensure(c, c->inv, (size_t)(inv_limit + 1) * 8))) return rc;
     if ((rc = ensure(c, c->invw, (size_t)invw_count * 16))) return rc;
-    const size_t need_pinned = (size_t)nq * 7 + 2;
+    const size_t need_pinned = (size_t)nq * (3 + kCountsPerQuery) + 2;
     if (c->pinned_cap < need_pinned) {
         if (c->capturing) return fail(DR_ERR_ARG, "internal: result buffer growth during graph capture");
         drop_graphs(c);
@@ -641,7 +641,7 @@ int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq,
     CU(record_event(c, 2));
     CU(cudaMemcpyAsync(c->queries.p, sq, (size_t)nq * sizeof(QueryDev), cudaMemcpyHostToDevice, c->stream));
     CU(cudaMemsetAsync(c->acc.p, 0, (size_t)nq * 3 * 8, c->stream));
-    CU(cudaMemsetAsync(c->counts.p, 0, (size_t)nq * 4 * 8, c->stream));
+    CU(cudaMemsetAsync(c->counts.p, 0, (size_t)nq * kCountsPerQuery * 8, c->stream));
     CU(cudaMemsetAsync(c->ticket.p, 0, 32, c->stream));
     if (sw)
         CU(cudaMemcpyAsync(c->witems.p, sw, witems.size() * sizeof(S1WinItem), cudaMemcpyHostToDevice, c->stream));
@@ -695,9 +695,10 @@ int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq,
     }
     CU(record_event(c, 4));
     CU(cudaMemcpyAsync(c->pinned, c->acc.p, (size_t)nq * 3 * 8, cudaMemcpyDeviceToHost, c->stream));
-    CU(cudaMemcpyAsync(c->pinned + (size_t)nq * 3, c->counts.p, (size_t)nq * 4 * 8, cudaMemcpyDeviceToHost,
+    CU(cudaMemcpyAsync(c->pinned + (size_t)nq * 3, c->counts.p, (size_t)nq * kCountsPerQuery * 8, cudaMemcpyDeviceToHost,
                        c->stream));
-    CU(cudaMemcpyAsync(c->pinned + (size_t)nq * 7, c->ticket.p, 16, cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaMemcpyAsync(c->pinned + (size_t)nq * (3 + kCountsPerQuery), c->ticket.p, 16, cudaMemcpyDeviceToHost,
+                       c->stream));
     CU(record_event(c, 5));
     *launches_out = launches;
     return DR_OK;
@@ -708,7 +709,7 @@ int finish_queries(dr_ctx* c, const int64_t* X, int64_t nq, int launches, size_t
                    dr_stats* st) {
     CU(cudaStreamSynchronize(c->stream));
     CU(cudaGetLastError());
-    if (c->pinned[(size_t)nq * 7 + 1])
+    if (c->pinned[(size_t)nq * (3 + kCountsPerQuery) + 1])
         return fail(DR_ERR_DEVICE, "sums kernel: op count of an evaluation disagreed with its plan");
     for (int64_t i = 0; i < nq; ++i) {
         uint64_t* a = c->pinned + 3 * i;
@@ -727,13 +728,15 @@ int finish_queries(dr_ctx* c, const int64_t* X, int64_t nq, int launches, size_t
         st->sieve_launches += 1;
         st->sums_launches += launches > 1 ? 1 : 0;
         st->h2d_bytes += (uint64_t)h2d_bytes;
-        st->d2h_bytes += (uint64_t)nq * 7 * 8 + 16;
+        st->d2h_bytes += (uint64_t)nq * (3 + kCountsPerQuery) * 8 + 16;
         const uint64_t* cnt = c->pinned + (size_t)nq * 3;
         for (int64_t i = 0; i < nq; ++i) {
-            st->terms += (int64_t)cnt[4 * i + 0];
-            st->evals += (int64_t)cnt[4 * i + 1];
-            st->s1_ops += cnt[4 * i + 2];
-            st->s2_ops += cnt[4 * i + 3];
+            const uint64_t* ci = cnt + (size_t)kCountsPerQuery * i;
+            st->terms += (int64_t)ci[0];
+            st->evals += (int64_t)ci[1];
+            st->s1_ops += ci[2];
+            st->s2_ops += ci[3];
+            st->s1_comp_ops += ci[4];
         }
         if (nq == 1) {
             st->C = c->pinned[0];

@@ -265,6 +265,19 @@ __device__ __forceinline__ void mark_item(uint32_t* buf32, const uint4 I, const 
     }
 }
 
+// The same marks from a known first hit at byte j0 (lane l takes j0 + l*m, then
+// every 32nd multiple): the odd-mode items whose first hit is carried across segments.
+__device__ __forceinline__ void mark_item_from(uint32_t* buf32, const uint4 I, uint32_t j0, int nb, int lane) {
+    const uint32_t m = I.x;
+    uint32_t j = j0 + (uint32_t)lane * m;
+    const uint32_t jend = min((uint32_t)nb, I.y + 1024u * m);
+    if (I.w >> 31) {
+        for (; j < jend; j += 32u * m) atomicOr(&buf32[j >> 2], 0x80u << ((j & 3) * 8));
+    } else {
+        for (; j < jend; j += 32u * m) atomicAdd(&buf32[j >> 2], I.z << ((j & 3) * 8));
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Segmented byte-log Mobius sieve + table outputs (ODD: odd values only).
 // ---------------------------------------------------------------------------
@@ -283,21 +296,48 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
     // with the modulus reciprocal -- in registers for every segment and reads them by
     // shuffles, instead of two dependent loads per item and segment (more items: the
     // loop from memory below).
+    //
+    // Odd mode carries each item's first hit from one segment of the CTA to its next
+    // one instead of recomputing it: consecutive segments of a CTA in the same tier lie
+    // D = gridDim.x * S values apart, the odd multiples of m are m bytes apart, so the
+    // first hit at or after byte I.y moves from b to (b - D/2) mod m.  myC holds
+    // (D/2) mod m; the first segment of the CTA and the first one after the dense /
+    // compressed boundary (where the bases stop being D apart) compute b afresh.
     uint4 myI = make_uint4(0u, 0xFFFFFFFFu, 0u, 0u);
     u64 myInv = 0;
+    uint32_t myB = 0, myC = 0;
     const bool ireg = a.n_items <= 32 * nwarps;
-    {
-        const int my_it = warp + nwarps * lane;
-        if (ireg && my_it < a.n_items) {
-            myI = __ldg(a.items + my_it);
+    const int my_it = warp + nwarps * lane;
+    const bool my_valid = ireg && my_it < a.n_items;
+    if (my_valid) {
+        myI = __ldg(a.items + my_it);
+        if (ODD) {
+            myC = (uint32_t)(((u64)gridDim.x * (u64)(a.S / 2)) % (u64)myI.x);
+        } else {
             const uint32_t pidx = myI.w & 0x7fffffffu;
             myInv = (myI.w >> 31) ? __ldg(a.sqinv + pidx) : __ldg(a.pinv + pidx);
         }
     }
     const int my_cnt = (ireg && a.n_items > warp) ? (a.n_items - warp + nwarps - 1) / nwarps : 0;
+    i64 prev_seg = -1;
     for (i64 seg = a.seg_begin + blockIdx.x; seg < a.seg_end; seg += gridDim.x) {
         const bool dense = seg < a.dense_segs;
         const i64 seg_base = dense ? seg * (i64)a.S : a.u_dense + (seg - a.dense_segs) * (i64)a.S;
+        if (ODD && my_valid) {
+            const uint32_t m = myI.x;
+            if (prev_seg >= 0 && (prev_seg < a.dense_segs) == dense) {
+                myB = myB >= myC ? myB - myC : myB + m - myC;
+            } else {
+                const uint32_t pidx = myI.w & 0x7fffffffu;
+                const u64 inv = (myI.w >> 31) ? __ldg(a.sqinv + pidx) : __ldg(a.pinv + pidx);
+                const u64 v0 = (u64)seg_base + 1 + 2ull * myI.y;  // the odd value of byte I.y
+                const uint32_t r = (uint32_t)umod_inv(v0, m, inv);
+                uint32_t d = r ? m - r : 0u;
+                if (d & 1u) d += m;
+                myB = d >> 1;
+            }
+        }
+        prev_seg = seg;
         const i64 seg_end = min(seg_base + (i64)a.S, dense ? a.u_dense : a.u_total);
         // Full mode sieves a segment in passes of S_sub values (the shared buffer holds
         // S_sub bytes), carrying the Mobius sum of the earlier passes into the outputs.
@@ -342,7 +382,12 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
             I.y = __shfl_sync(0xffffffffu, myI.y, k);
             I.z = __shfl_sync(0xffffffffu, myI.z, k);
             I.w = __shfl_sync(0xffffffffu, myI.w, k);
-            if (I.y < (uint32_t)nb) mark_item<ODD>(buf32, I, __shfl_sync(0xffffffffu, myInv, k), low, nb, lane);
+            if (ODD) {
+                const uint32_t b = __shfl_sync(0xffffffffu, myB, k);
+                if (I.y < (uint32_t)nb) mark_item_from(buf32, I, I.y + b, nb, lane);
+            } else {
+                if (I.y < (uint32_t)nb) mark_item<ODD>(buf32, I, __shfl_sync(0xffffffffu, myInv, k), low, nb, lane);
+            }
         }
         for (int it = warp; it < (ireg ? 0 : a.n_items); it += nwarps) {
             const uint4 I = __ldg(a.items + it);
@@ -524,8 +569,10 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
                         dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
                         dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
                     } else {
-                        for (int b = 0; b < len - 16 * g; ++b)
-                            out[16 * g + b] = (int16_t)((pk[b >> 1] >> (16 * (b & 1))) & 0xFFFFu);
+                        const int rem = len - 16 * g;  // fewer than 16 values left: constant indices
+#pragma unroll
+                        for (int b = 0; b < 16; ++b)
+                            if (b < rem) out[16 * g + b] = (int16_t)((pk[b >> 1] >> (16 * (b & 1))) & 0xFFFFu);
                     }
                 }
             } else {
@@ -566,8 +613,10 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
                         dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
                         dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
                     } else {
-                        for (int b = 0; b < len - 16 * g; ++b)
-                            out[16 * g + b] = (int16_t)((pk[b >> 1] >> (16 * (b & 1))) & 0xFFFFu);
+                        const int rem = len - 16 * g;  // fewer than 16 values left: constant indices
+#pragma unroll
+                        for (int b = 0; b < 16; ++b)
+                            if (b < rem) out[16 * g + b] = (int16_t)((pk[b >> 1] >> (16 * (b & 1))) & 0xFFFFu);
                     }
                 }
             }
@@ -844,46 +893,88 @@ __device__ __forceinline__ int query_of_slot(const QueryDev* q, int nq, u64 s) {
     return lo;
 }
 
-// counts[4*q + 0..3]: terms, evaluations, S1 lookups, S2 wheel positions
+// S1 lookups of an evaluation whose quotient y/n lies in the compressed tier
+// (q > u_dense, i.e. n <= y/(u_dense+1)): a prefix of each S1 segment's divisors.
+__device__ __forceinline__ u64 s1_compressed_lookups(const EvalDesc& d, const TableView& T) {
+    const i64 nc = (i64)udiv(d.y, (u64)T.u_dense + 1);  // largest n with y/n > u_dense
+    u64 tot = 0;
+    for (int g = 0; g < kS1Seg; ++g) {
+        const i64 cnt = d.s1_full[g], n0 = d.s1_n0[g];
+        if (cnt <= 0) continue;
+        const int st = d.s1_stride[g];
+        i64 k;
+        if (st == S1_WHEEL) k = nc >= 1 ? wheel_upper(nc) - n0 + 1 : 0;
+        else k = nc >= n0 ? (nc - n0) / st + 1 : 0;
+        tot += (u64)max(0ll, min(k, cnt));
+    }
+    return tot;
+}
+
+// counts[kCountsPerQuery*q + 0..4]: terms, evaluations, S1 lookups, S2 wheel
+// positions, compressed-tier S1 lookups -- summed over the warp before the atomics
 __global__ void plan_kernel(const QueryDev* __restrict__ qs, int nq, const TableView T, u64 n_slots,
                             u64* __restrict__ ops, u64* __restrict__ acc, i64* __restrict__ counts,
                             S1WinDesc* __restrict__ wdesc) {
+    // whole warps step together (the stride is a multiple of 32), so the counters
+    // can be summed over the warp with every lane taking part
     const u64 stride = (u64)gridDim.x * blockDim.x;
-    for (u64 s = (u64)blockIdx.x * blockDim.x + threadIdx.x; s < n_slots; s += stride) {
-        const int qi = query_of_slot(qs, nq, s);
-        const QueryDev Q = qs[qi];
-        const u64 local = s - Q.slot_base;
-        EvalDesc d;
-        decode_eval(Q, T, (i64)(local >> 1), (int)(local & 1), d);
-        ops[s] = d.total;
-        if (wdesc && Q.win) {
-            S1WinDesc w;
-            w.y = d.y;
-            for (int g = 0; g < kS1Seg; ++g) {
-                const bool on = d.kind != EVAL_NONE && d.s1_full[g] > 0 && d.s1_wc[g] > 0;
-                w.n0[g] = on ? (uint32_t)d.s1_n0[g] : 0u;
-                w.cnt[g] = on ? (uint32_t)d.s1_full[g] : 0u;
-                w.wc[g] = on ? (uint32_t)d.s1_wc[g] : 0u;
-                w.w0[g] = on ? (uint32_t)(udiv(d.y, s1_n_at(d.s1_n0[g], d.s1_stride[g], (u64)(d.s1_full[g] - 1))) /
-                                          Q.win)
-                             : 0u;
-                w.sg[g] = on ? (int32_t)(d.coef * d.s1_sign[g]) * d.s1_stride[g] : 0;
+    const int lane = threadIdx.x & 31;
+    for (u64 s0 = (u64)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); s0 < n_slots; s0 += stride) {
+        const u64 s = s0 + (u64)lane;
+        const bool valid = s < n_slots;
+        const int qi = query_of_slot(qs, nq, valid ? s : n_slots - 1);
+        u64 v[6] = {0, 0, 0, 0, 0, 0};  // C, terms, evaluations, S1, S2, compressed S1
+        if (valid) {
+            const QueryDev Q = qs[qi];
+            const u64 local = s - Q.slot_base;
+            EvalDesc d;
+            decode_eval(Q, T, (i64)(local >> 1), (int)(local & 1), d);
+            ops[s] = d.total;
+            if (wdesc && Q.win) {
+                S1WinDesc w;
+                w.y = d.y;
+                for (int g = 0; g < kS1Seg; ++g) {
+                    const bool on = d.kind != EVAL_NONE && d.s1_full[g] > 0 && d.s1_wc[g] > 0;
+                    w.n0[g] = on ? (uint32_t)d.s1_n0[g] : 0u;
+                    w.cnt[g] = on ? (uint32_t)d.s1_full[g] : 0u;
+                    w.wc[g] = on ? (uint32_t)d.s1_wc[g] : 0u;
+                    w.w0[g] = on ? (uint32_t)(udiv(d.y, s1_n_at(d.s1_n0[g], d.s1_stride[g], (u64)(d.s1_full[g] - 1))) /
+                                              Q.win)
+                                 : 0u;
+                    w.sg[g] = on ? (int32_t)(d.coef * d.s1_sign[g]) * d.s1_stride[g] : 0;
+                }
+                wdesc[s] = w;
             }
-            wdesc[s] = w;
+            if (d.kind != EVAL_NONE) {
+                v[0] = (u64)(d.coef * eval_constant(d, T));
+                v[1] = (local & 1) == 0 ? 1 : 0;
+                v[2] = 1;
+                u64 s1d = 0, s1f = 0;  // lookups left to the sums kernel, all lookups
+                for (int g = 0; g < kS1Seg; ++g) {
+                    s1d += (u64)d.s1_cnt[g];
+                    s1f += (u64)d.s1_full[g];
+                }
+                v[3] = s1f;
+                v[4] = d.total - s1d;
+                v[5] = s1_compressed_lookups(d, T);
+            }
         }
-        if (d.kind != EVAL_NONE) {
-            const i64 c = d.coef * eval_constant(d, T);
-            atomicAdd(acc + 3 * qi, (u64)c);
-            unsigned long long* cq = reinterpret_cast<unsigned long long*>(counts + 4 * qi);
-            if ((local & 1) == 0) atomicAdd(cq + 0, 1ull);
-            atomicAdd(cq + 1, 1ull);
-            u64 s1d = 0, s1f = 0;  // lookups left to the sums kernel, all lookups
-            for (int g = 0; g < kS1Seg; ++g) {
-                s1d += (u64)d.s1_cnt[g];
-                s1f += (u64)d.s1_full[g];
+        // one atomic per counter and warp where all its slots belong to one query
+        const int q0 = __shfl_sync(0xffffffffu, qi, 0);
+        if (__all_sync(0xffffffffu, qi == q0)) {
+#pragma unroll
+            for (int i = 0; i < 6; ++i) v[i] = warp_sum_u64(v[i]);
+            if (lane == 0) {
+                atomicAdd(acc + 3 * qi, v[0]);
+                unsigned long long* cq = reinterpret_cast<unsigned long long*>(counts + kCountsPerQuery * qi);
+                for (int i = 0; i < 5; ++i)
+                    if (v[i + 1]) atomicAdd(cq + i, v[i + 1]);
             }
-            atomicAdd(cq + 2, s1f);
-            atomicAdd(cq + 3, d.total - s1d);
+        } else if (valid) {
+            if (v[0]) atomicAdd(acc + 3 * qi, v[0]);
+            unsigned long long* cq = reinterpret_cast<unsigned long long*>(counts + kCountsPerQuery * qi);
+            for (int i = 0; i < 5; ++i)
+                if (v[i + 1]) atomicAdd(cq + i, v[i + 1]);
         }
     }
 }

@@ -126,6 +126,10 @@ size_t sieve_smem_bytes(int S, bool odd);
 void launch_seg_scan(const int32_t* in, int32_t* out, i64 n, cudaStream_t s);
 void launch_fixup(int16_t* dM, i64 u_dense, int S, const int32_t* seg_off, int32_t* ckpt, i64 nwords,
                   i64 dense_segs, int sm_count, cudaStream_t s);
+// Per-query counters written by plan_kernel: counts[kCountsPerQuery*q + 0..4] =
+// outer terms, evaluations, S1 lookups, S2 wheel positions, and the S1 lookups
+// whose quotient lies in the compressed tier (q > u_dense).
+constexpr int kCountsPerQuery = 5;
 void launch_plan(const QueryDev* q, int nq, const TableView& T, u64 n_slots, u64* ops, u64* acc,
                  i64* counts, S1WinDesc* wdesc, int sm_count, cudaStream_t s);
 // Windowed S1 (window length win: a power of two, 2^12 .. 2^16).

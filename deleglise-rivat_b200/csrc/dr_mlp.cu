@@ -228,7 +228,7 @@ static void outputs_to_params(int64_t X, const float yn[kOut], dr_params* p) {
     const double lxc = std::min(kLog10XMax, std::max(kLog10XMin, lx));
     const double cap = std::exp2(std::min(41.0, std::max(20.0, (double)o[2]))) * std::pow(10.0, (2.0 / 3.0) * (lx - lxc));
     int seg = (int)std::lround(o[3]);
-    seg = std::max(12, std::min(seg, 17));
+    seg = std::max(12, std::min(seg, 18));
     params_clear(p);
     const double loglogX = std::log(std::max(2.0, std::log((double)X)));
     int64_t u = (int64_t)std::min(cap, fx * std::pow((double)X / loglogX, 2.0 / 3.0));
@@ -238,7 +238,9 @@ static void outputs_to_params(int64_t X, const float yn[kOut], dr_params* p) {
     u = ((u + 255) / 256) * 256;
     const int64_t e256 = (endpoint + 255) & ~255LL;
     p->u_total = u;
-    p->u_dense = std::min(u, std::max(e256, std::min<int64_t>(128000000LL, ((u / 4 + 255) & ~255LL))));
+    // dense int16 tier as in the B200 policy: max(1.28e8, u/16) values, at most 4e9
+    const int64_t dense_target = std::min<int64_t>(4000000000LL, std::max<int64_t>(128000000LL, u / 16));
+    p->u_dense = std::min<int64_t>(u, std::max<int64_t>(e256, (dense_target + 255) & ~255LL));
     p->cx = cx;
     p->mu_limit = std::min(u, std::max(endpoint, X / u + 1000));
     p->segment_log2 = seg;

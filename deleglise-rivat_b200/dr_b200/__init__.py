@@ -83,6 +83,7 @@ class Stats(ctypes.Structure):
         ("reserved", ctypes.c_int32),
         ("h2d_bytes", ctypes.c_uint64),
         ("d2h_bytes", ctypes.c_uint64),
+        ("s1_comp_ops", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:

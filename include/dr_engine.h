@@ -81,6 +81,7 @@ typedef struct {
     int32_t sieve_launches, sums_launches, kernel_launches;
     int32_t reserved;
     uint64_t h2d_bytes, d2h_bytes; /* host<->device bytes copied by the call   */
+    uint64_t s1_comp_ops;    /* S1 lookups in the compressed tier (q > u_dense) */
 } dr_stats;
 
 typedef struct {

@@ -167,3 +167,19 @@ def test_windowed_s1_matches_direct(engine):
     p = dr_b200.default_params(X, dr_b200.POLICY_GPU)
     small = dr_b200.Params(**{**p.as_dict(), "u_dense": 40000, "s1_window_log2": 15})
     assert engine.mertens(X, small).M == 62366
+
+
+def test_compressed_lookup_counter(engine):
+    """s1_comp_ops counts the S1 lookups whose quotient lies above the dense tier:
+    none with an all-dense table, all of them with no dense tier, in between
+    otherwise, and M(X) is the same in all three."""
+    X = 10**12
+    p = dr_b200.default_params(X, dr_b200.POLICY_COMPRESSED)
+    dense = dr_b200.Params(**{**p.as_dict(), "u_dense": p.u_total})
+    none = dr_b200.Params(**{**p.as_dict(), "u_dense": 0})
+    r_all, r_none, r_mid = engine.mertens(X, dense), engine.mertens(X, none), engine.mertens(X, p)
+    assert r_all.M == r_none.M == r_mid.M == 62366
+    assert r_all.stats.s1_comp_ops == 0
+    assert r_none.stats.s1_comp_ops == r_none.stats.s1_ops > 0
+    assert 0 < r_mid.stats.s1_comp_ops < r_mid.stats.s1_ops
+    assert r_all.stats.s1_ops == r_none.stats.s1_ops == r_mid.stats.s1_ops
