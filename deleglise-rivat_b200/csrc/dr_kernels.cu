@@ -307,7 +307,10 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
     u64 myInv = 0;
     uint32_t myB = 0, myC = 0;
     const bool ireg = a.n_items <= 32 * nwarps;
-    const int my_it = warp + nwarps * lane;
+    // lane k of warp w holds item nwarps*k + w (k even) or nwarps*k + nwarps-1-w (k odd):
+    // items are sorted by modulus, so the heavy ones of each round of nwarps items
+    // alternate between the first and the last warps
+    const int my_it = nwarps * lane + ((lane & 1) ? nwarps - 1 - warp : warp);
     const bool my_valid = ireg && my_it < a.n_items;
     if (my_valid) {
         myI = __ldg(a.items + my_it);
@@ -318,7 +321,7 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
             myInv = (myI.w >> 31) ? __ldg(a.sqinv + pidx) : __ldg(a.pinv + pidx);
         }
     }
-    const int my_cnt = (ireg && a.n_items > warp) ? (a.n_items - warp + nwarps - 1) / nwarps : 0;
+    const int my_cnt = __popc(__ballot_sync(0xffffffffu, my_valid));  // valid items are a prefix of the lanes
     i64 prev_seg = -1;
     for (i64 seg = a.seg_begin + blockIdx.x; seg < a.seg_end; seg += gridDim.x) {
         const bool dense = seg < a.dense_segs;
@@ -424,7 +427,11 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
             }
         }
         //    Offsets low mod p: on the 32-bit quotient route (qest/qfix) while
-        //    p <= low and low/p < 2^31, else from the 64-bit reciprocal.
+        //    p <= low and low/p < 2^31, else from the 64-bit reciprocal.  Round k
+        //    gives thread t the prime T*k + t (k even) or T*k + T-1-t (k odd): the
+        //    small primes of each round (the most hits) alternate between the
+        //    first and the last warps, which evens out the warps' marking before
+        //    the barrier.
         const double lowd = __ull2double_rn((u64)low);
         uint32_t p_n = 0;
         double rc_n = 0.0;
@@ -432,12 +439,13 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
             p_n = __ldg(a.primes + a.tierB_first + tid);
             if (a.prcp) rc_n = __ldg(a.prcp + a.tierB_first + tid);
         }
-        for (int i = a.tierB_first + tid; i < a.n_primes; i += T) {
+        for (int k = 0, i = a.tierB_first + tid; i < a.n_primes; ++k) {
             const uint32_t p = p_n;  // loaded one iteration ahead
             const double rc = rc_n;
-            if (i + T < a.n_primes) {
-                p_n = __ldg(a.primes + i + T);
-                if (a.prcp) rc_n = __ldg(a.prcp + i + T);
+            const int inext = a.tierB_first + T * (k + 1) + ((k & 1) ? tid : T - 1 - tid);
+            if (inext < a.n_primes) {
+                p_n = __ldg(a.primes + inext);
+                if (a.prcp) rc_n = __ldg(a.prcp + inext);
             }
             const uint32_t w = (32u - __clz(p - 1)) | 1u;
             uint32_t r;
@@ -449,6 +457,7 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
             if (ODD && (d & 1u)) d += p;
             for (uint32_t j = ODD ? d >> 1 : d; j < (uint32_t)nb; j += p)
                 atomicAdd(&buf32[j >> 2], w << ((j & 3) * 8));
+            i = inext;
         }
         __syncthreads();
 
@@ -849,13 +858,13 @@ void launch_seg_scan(const int32_t* in, int32_t* out, i64 n, cudaStream_t s) {
     seg_scan_kernel<<<1, 1024, 0, s>>>(in, out, n);
 }
 
-__global__ void fixup_kernel(int16_t* dM, i64 u_dense, int S, const int32_t* seg_off, int32_t* ckpt, i64 nwords,
+__global__ void fixup_kernel(int16_t* dM, i64 u_dense, int lgS, const int32_t* seg_off, int32_t* ckpt, i64 nwords,
                              i64 dense_segs) {
     const i64 stride = (i64)gridDim.x * blockDim.x;
     const i64 t0 = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     const i64 n8 = (u_dense + 7) / 8;
     for (i64 i = t0; i < n8; i += stride) {
-        const int32_t off = seg_off[(8 * i) / S];
+        const int32_t off = seg_off[(8 * i) >> lgS];
         if (8 * i + 8 <= u_dense) {
             uint4* p = reinterpret_cast<uint4*>(dM) + i;
             uint4 v = *p;
@@ -869,15 +878,17 @@ __global__ void fixup_kernel(int16_t* dM, i64 u_dense, int S, const int32_t* seg
             for (i64 k = 8 * i; k < u_dense; ++k) dM[k] = (int16_t)(dM[k] + off);
         }
     }
-    for (i64 w = t0; w < nwords; w += stride) ckpt[w] += seg_off[dense_segs + (64 * w) / S];
+    for (i64 w = t0; w < nwords; w += stride) ckpt[w] += seg_off[dense_segs + ((64 * w) >> lgS)];
 }
 
 void launch_fixup(int16_t* dM, i64 u_dense, int S, const int32_t* seg_off, int32_t* ckpt, i64 nwords,
                   i64 dense_segs, int sm_count, cudaStream_t s) {
     const i64 work = max((u_dense + 7) / 8, nwords);
     if (work <= 0) return;
+    int lgS = 0;  // S is a power of two (2^12 .. 2^18)
+    while ((1 << lgS) < S) ++lgS;
     const int grid = (int)std::min<i64>((work + 255) / 256, (i64)sm_count * 8);
-    fixup_kernel<<<grid, 256, 0, s>>>(dM, u_dense, S, seg_off, ckpt, nwords, dense_segs);
+    fixup_kernel<<<grid, 256, 0, s>>>(dM, u_dense, lgS, seg_off, ckpt, nwords, dense_segs);
 }
 
 // ---------------------------------------------------------------------------
