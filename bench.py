@@ -408,7 +408,14 @@ def run_engine(args, world, rank, local):
         xs = batch_inputs()
 
         def batch_time(bp, reps=3):
+            """(replay seconds per batch, results, replay stats, first-call seconds):
+            the first call of a new batch runs eagerly and captures the graph (host
+            wall time, synchronised); identical calls then replay it."""
+            torch.cuda.synchronize()
+            f0 = time.perf_counter()
             got, _ = eng.mertens_batch(xs, bp)  # eager run; captures the graph
+            torch.cuda.synchronize()
+            first = time.perf_counter() - f0
             t0 = torch.cuda.Event(enable_timing=True)
             t1 = torch.cuda.Event(enable_timing=True)
             t0.record(stream)
@@ -416,13 +423,13 @@ def run_engine(args, world, rank, local):
                 got, bst = eng.mertens_batch(xs, bp)  # graph replays
             t1.record(stream)
             torch.cuda.synchronize()
-            return t0.elapsed_time(t1) / 1e3 / reps, got, bst
+            return t0.elapsed_time(t1) / 1e3 / reps, got, bst, first
 
-        untuned_s, _, _ = batch_time([dr_b200.default_params(x, dr_b200.POLICY_GPU) for x in xs])
+        untuned_s, _, _, _ = batch_time([dr_b200.default_params(x, dr_b200.POLICY_GPU) for x in xs])
         tt0 = time.perf_counter()
         bp, _ = eng.autotune_batch(xs, 24)
         tune_s = time.perf_counter() - tt0
-        bs, got, bst = batch_time(bp)
+        bs, got, bst, first_s = batch_time(bp)
         # baseline: 256 sequential plain single-query calls with default parameters
         s0 = torch.cuda.Event(enable_timing=True)
         s1 = torch.cuda.Event(enable_timing=True)
@@ -433,9 +440,13 @@ def run_engine(args, world, rank, local):
         ss = s0.elapsed_time(s1) / 1e3
         if seq != got:
             raise SystemExit("batched and single-query results differ")
+        kern_ms = bst.table_ms + bst.plan_ms + bst.sums_ms
         batch = {"queries": len(xs), "M_per_s": len(xs) / bs, "s_per_batch": bs,
+                 "replay_M_per_s": len(xs) / bs, "first_call_s": first_s,
+                 "first_call_M_per_s": len(xs) / first_s,
                  "sequential_plain_M_per_s": len(xs) / ss, "speedup_vs_sequential": ss / bs,
                  "untuned_batch_M_per_s": len(xs) / untuned_s, "launches_per_batch": bst.kernel_launches,
+                 "replay_kernel_ms": kern_ms, "replay_gap_ms": bs * 1e3 - kern_ms,
                  "cuda_graph": True,
                  "autotune": {"seconds": tune_s, "u_total": bp[0].u_total, "cx": bp[0].cx,
                               "segment_log2": bp[0].segment_log2, "block_threads": bp[0].block_threads,
