@@ -14,12 +14,15 @@ the reference's own CPU engine (oracle/_ref, built from its sources) on this
 host's cores.
 
 Besides the contract's keys the line carries `phases_ms` (table, planning,
-sums), `roofline` (the S1/S2 phase against the HBM copy peak), `int_peaks`
-(shared-memory atomic, IMAD and DFMA ceilings measured on this GPU by
-dr_measure_peaks), `table_roofline` (the sieve's atomics per second against
-those ceilings and the table writes against HBM), `default_params` and
-`learned_tuner` (the same step with the reference's parameters and with the
-learned tuner's proposal) and `batched` (the 256-query batch).
+sums), `roofline` (the S1/S2 phase: against the HBM copy peak on its
+algorithmic bytes, and in `roofline.issue` against its binding unit,
+instruction issue), `table_roofline` (the table phase against instruction
+issue, with the sieve's shared-memory atomics and the table's HBM writes
+beside it), `int_peaks` (shared-memory atomic, IMAD and DFMA ceilings measured
+on this GPU by dr_measure_peaks), `default_params` and `learned_tuner` (the
+same step with the reference's parameters and with the learned tuner's
+proposal) and `batched` (the 256-query batch: replay throughput, first-call
+cost, launches per batch).
 """
 from __future__ import annotations
 
@@ -234,18 +237,17 @@ def sieve_marks(u_total, u_dense, sm_count, S=1 << 17):
 
 
 # Warp instructions per unit of work, from ncu smsp__inst_executed.sum of one launch
-# divided by that launch's work (the captures run at M(10^15) and on the M(10^15)
-# table; the mix per op is set by the per-lookup / per-position / per-value code):
-#   sums_kernel: per S1 lookup and per S2 wheel position (split by the two
-#     timing-only captures that keep one of the two parts, whose sum matches the
-#     whole kernel's count within 2%);
-#   sieve_kernel (odd mode): per table value.
-SUMS_INST_PER_S1 = 0.68
-SUMS_INST_PER_S2 = 1.57
-SIEVE_INST_PER_VALUE = 1.0
-# DRAM bytes per op of sums_kernel (dram__bytes_read.sum + dram__bytes_write.sum of
-# one launch over its S1 lookups + S2 positions) at M(10^15) ...
-SUMS_DRAM_PER_OP = 1.05
+# divided by that launch's work:
+#   sums_kernel at M(10^15) (B200 policy): 8.44e9 instructions for 6.50e9 S1 lookups +
+#     2.82e9 S2 wheel positions, split between the two in the ratio of the earlier
+#     timing-only captures that keep one of the two parts (0.68 : 1.57);
+#   sieve_kernel, odd mode, on the M(10^15) table: 6.56e7 instructions for 1.01e8 values.
+SUMS_INST_PER_S1 = 0.65
+SUMS_INST_PER_S2 = 1.50
+SIEVE_INST_PER_VALUE = 0.65
+# DRAM bytes per op of sums_kernel (dram__bytes_read.sum + dram__bytes_write.sum of one
+# launch over its S1 lookups + S2 positions) at M(10^15): 11.36 GB / 9.32e9 ops.
+SUMS_DRAM_PER_OP = 1.22
 
 
 def sums_roofline(st, sums_ms, peak, peak_kind, issue_peak, f_mhz):
@@ -285,7 +287,7 @@ def sieve_roofline(p, tab_ms, peak, peaks_int, issue_peak, sms):
         "bound": "instruction issue", "achieved": inst / t, "peak": issue_peak, "unit": "warp instructions/s",
         "frac": inst / t / issue_peak,
         "basis": f"{SIEVE_INST_PER_VALUE} warp instructions per table value (ncu, odd-mode sieve on the "
-                 f"M(10^15) table); peak = SMs x 4 x SM clock",
+                 f"M(10^15) table); peak = SMs x 4 x the median SM clock of the timed region",
         "atomics": {"marks": marks, "achieved": marks / t, "peak": peaks_int["smem_atomic_per_s"],
                     "peak_sieve_pattern": peaks_int["smem_atomic_stride_per_s"], "unit": "atomics/s",
                     "frac": marks / t / peaks_int["smem_atomic_per_s"],
