@@ -190,6 +190,11 @@ __device__ __forceinline__ void planes_odd_mode(const SieveArgs& a, const uint32
     const uint32_t rot = (uint32_t)(lane >> 2) & 7u;
     const uint32_t* src = buf32 + 8 * w;
     const bool full = 8 * w + 8 <= nw16;
+    // nearly every word: all 32 bytes sieved, none at or across the power-of-two edge,
+    // so one constant k serves the whole word and no byte needs a mask
+    const i64 b0 = 32 * (i64)w;
+    const bool simple = fz.on && full && b0 + 32 <= fz.nb && (b0 + 32 <= fz.edge || b0 >= fz.edge);
+    const uint32_t kw = b0 + 32 <= fz.edge ? fz.kbelow : fz.kabove;
     uint32_t zl = 0, zh = 0, gl = 0, gh = 0;
 #pragma unroll
     for (int t = 0; t < 8; ++t) {
@@ -197,7 +202,11 @@ __device__ __forceinline__ void planes_odd_mode(const SieveArgs& a, const uint32
         const int idx = 8 * w + (int)tt;
         const uint32_t v = (full || idx < nw16) ? src[tt] : 0u;
         uint32_t nzb, ngb;
-        if (fz.on && idx != fz.skip) {
+        if (simple) {
+            const uint32_t x = ((((v & 0x7F7F7F7Fu) + kw) >> 7) ^ v) & 0x01010101u;
+            nzb = ~(v >> 7) & 0x01010101u;
+            ngb = nzb & ~x;
+        } else if (fz.on && idx != fz.skip) {
             const i64 j0 = 4 * (i64)idx;
             const uint32_t s = (v & 0x7F7F7F7Fu) + (j0 < fz.edge ? fz.kbelow : fz.kabove);
             const uint32_t x = ((s >> 7) ^ v) & 0x01010101u;  // 1: mu = +1 (if not flagged)
@@ -245,6 +254,29 @@ __device__ __forceinline__ void planes_odd_mode(const SieveArgs& a, const uint32
     *neg = g;
 }
 
+// Marks of one warp item I from its first hit at byte j0 (lane l takes j0 + l*m, then
+// every 32nd multiple, up to the item's 1024 hits or the end of the sieved bytes).
+// A lane's strides are 32*m bytes, a multiple of 4: its byte position within the
+// 32-bit word, and so the shifted mark, stays the same, and the word advances by 8*m.
+__device__ __forceinline__ void mark_item_from(uint32_t* buf32, const uint4 I, uint32_t j0, int nb, int lane) {
+    const uint32_t m = I.x;
+    const uint32_t j = j0 + (uint32_t)lane * m;
+    const uint32_t jend = min((uint32_t)nb, I.y + 1024u * m);
+    const uint32_t ph = j & 3u;
+    // byte 4*(p - buf32) + ph < jend  <=>  p - buf32 < (jend - ph + 3) / 4
+    const uint32_t wend = jend + 3u >= ph ? (jend + 3u - ph) >> 2 : 0u;
+    uint32_t* p = buf32 + (j >> 2);
+    uint32_t* const pend = buf32 + wend;
+    if (I.w >> 31) {
+        const uint32_t v = 0x80u << (8u * ph);
+        for (; p < pend; p += 8u * m) atomicOr(p, v);
+    } else {
+        const uint32_t v = I.z << (8u * ph);
+        for (; p < pend; p += 8u * m) atomicAdd(p, v);
+    }
+}
+
+
 // Marks of one warp item I = {modulus m, first byte, weight or 0x80, prime index |
 // square bit 31}: lanes stride the multiples of m at or after byte I.y (ODD: the odd
 // multiples, m bytes apart), 32 strides each, with the 64-bit reciprocal inv of m.
@@ -256,26 +288,7 @@ __device__ __forceinline__ void mark_item(uint32_t* buf32, const uint4 I, const 
     const uint32_t r = (uint32_t)umod_inv(v0, m, inv);
     uint32_t d = r ? m - r : 0u;  // first multiple: v0 + d
     if (ODD && (d & 1u)) d += m;  // v0 is odd: the first odd multiple
-    uint32_t j = I.y + (ODD ? d >> 1 : d) + (uint32_t)lane * m;
-    const uint32_t jend = min((uint32_t)nb, I.y + 1024u * m);
-    if (I.w >> 31) {
-        for (; j < jend; j += 32u * m) atomicOr(&buf32[j >> 2], 0x80u << ((j & 3) * 8));
-    } else {
-        for (; j < jend; j += 32u * m) atomicAdd(&buf32[j >> 2], I.z << ((j & 3) * 8));
-    }
-}
-
-// The same marks from a known first hit at byte j0 (lane l takes j0 + l*m, then
-// every 32nd multiple): the odd-mode items whose first hit is carried across segments.
-__device__ __forceinline__ void mark_item_from(uint32_t* buf32, const uint4 I, uint32_t j0, int nb, int lane) {
-    const uint32_t m = I.x;
-    uint32_t j = j0 + (uint32_t)lane * m;
-    const uint32_t jend = min((uint32_t)nb, I.y + 1024u * m);
-    if (I.w >> 31) {
-        for (; j < jend; j += 32u * m) atomicOr(&buf32[j >> 2], 0x80u << ((j & 3) * 8));
-    } else {
-        for (; j < jend; j += 32u * m) atomicAdd(&buf32[j >> 2], I.z << ((j & 3) * 8));
-    }
+    mark_item_from(buf32, I, I.y + (ODD ? d >> 1 : d), nb, lane);
 }
 
 // ---------------------------------------------------------------------------
