@@ -26,6 +26,7 @@ typedef long long i64;
 // integer arithmetic decides.
 // ---------------------------------------------------------------------------
 
+#ifdef __CUDACC__
 // 1/d rounded down with margin: RU conversion makes fd >= d, rcp.approx is
 // within a few ulp of 1/fd, and the (1 - 2^-17) factor absorbs that error.
 __device__ __forceinline__ float rcp_floor_estimate(uint32_t d) {
@@ -60,6 +61,8 @@ __device__ __forceinline__ u64 udiv_rcp(u64 y, double yd, uint32_t n, double r) 
     return qe + (u64)(i64)((int)(rem >= (i64)n) - (int)(rem < 0));
 }
 
+#endif  // __CUDACC__
+
 // 32-bit quotients of the S1 / S2 fast paths (n < 2^31 and floor(y/n) < 2^31).
 // qest: ceil(yd*r - 1/2) read from the low mantissa word of RU(yd*r + 2^52 - 1/2)
 // (one FMA; for y >= n the sum lies in [2^52, 2^53), where the spacing is 1).  yd*r
@@ -69,6 +72,7 @@ __device__ __forceinline__ u64 udiv_rcp(u64 y, double yd, uint32_t n, double r) 
 // say which one (n < 2^31); one IMAD and a sign bit replace the 64-bit remainder.
 constexpr double kQBias = 4503599627370495.5;  // 2^52 - 1/2
 
+#ifdef __CUDACC__
 __device__ __forceinline__ uint32_t qest(double yd, double r) {
     return (uint32_t)__double2loint(__fma_ru(yd, r, kQBias));
 }
@@ -83,6 +87,8 @@ __device__ __forceinline__ u64 udiv(u64 y, u64 d) {
     if ((y >> 32) == 0) return (uint32_t)y / (uint32_t)d;
     return udiv_u64_u32(y, (uint32_t)d, rcp_floor_estimate((uint32_t)d));
 }
+
+#endif  // __CUDACC__
 
 // ---------------------------------------------------------------------------
 // S2 summands (mertens_dr.hpp:462-482 tabulates them; here they come from
@@ -126,6 +132,7 @@ __host__ __device__ constexpr PieceCoef make_piece_coef(int piece) {
     return c;
 }
 
+#ifdef __CUDACC__
 __device__ __forceinline__ i64 piece_eval(const PieceCoef& c, u64 q) {
     u64 k;
     uint32_t r;
@@ -140,6 +147,8 @@ __device__ __forceinline__ i64 piece_eval(const PieceCoef& c, u64 q) {
     const int t = (int)((c.packed >> (5 * r)) & 31u) - 16;
     return c.a * (i64)k + t;
 }
+
+#endif  // __CUDACC__
 
 // ---------------------------------------------------------------------------
 // Tables in HBM.
@@ -161,6 +170,7 @@ struct TableView {
     i64 u_dense, u_total, mu_limit;
 };
 
+#ifdef __CUDACC__
 __device__ __forceinline__ int32_t table_M(const TableView& t, u64 q) {
     if (q <= (u64)t.u_dense) return q ? (int32_t)__ldg(t.dM + (q - 1)) : 0;
     const u64 off = q - (u64)t.u_dense - 1;
@@ -181,6 +191,8 @@ __device__ __forceinline__ int wheel_mu(const uint4* wheel, u64 j) {
     return ((nz >> b) & 1u) ? (((ng >> b) & 1u) ? -1 : 1) : 0;
 }
 
+#endif  // __CUDACC__
+
 // ---------------------------------------------------------------------------
 // One query of a (possibly batched) launch.
 // ---------------------------------------------------------------------------
@@ -200,6 +212,7 @@ struct QueryDev {
 #define DRB_WIN_MIN 64  // lookups of a segment in its last window (a power of two)
 #endif
 
+#ifdef __CUDACC__
 // Windowed S1 (s1win_kernel): the S1 lookups M(q) of an S1 segment with q below a
 // cut are summed window by window (q in [w*W, (w+1)*W), the window of the M table in
 // shared memory), the ones above it by the sums kernel.  The cut, a multiple of W,
@@ -229,6 +242,8 @@ __device__ __forceinline__ i64 split_point(double cx, i64 y) {
 // Outer candidate c -> k: 1, 5, 7, 11, ... (k coprime to 6).
 __device__ __forceinline__ i64 candidate_k(i64 c) { return 3 * c + 1 + (c & 1); }
 
+#endif  // __CUDACC__
+
 enum { EVAL_NONE = 0, EVAL_SINGLE = 1, EVAL_COMB2 = 2 };
 
 // S1 segments: arithmetic progressions n = n0 + stride*i (stride 1, 2 or 6), or,
@@ -237,6 +252,7 @@ enum { EVAL_NONE = 0, EVAL_SINGLE = 1, EVAL_COMB2 = 2 };
 constexpr int kS1Seg = 4;
 enum { S1_WHEEL = 3 };
 
+#ifdef __CUDACC__
 __device__ __forceinline__ u64 s1_n_at(i64 n0, int st, u64 i) {
     return st == S1_WHEEL ? (u64)candidate_k(n0 + (i64)i) : (u64)n0 + (u64)st * i;
 }
@@ -250,6 +266,8 @@ __device__ __forceinline__ i64 wheel_upper(i64 n) {
     const i64 c = (n - 1) / 3;
     return c - (candidate_k(c) > n ? 1 : 0);
 }
+
+#endif  // __CUDACC__
 
 // Index ranges of one evaluation in op order: S1 segments first, then S2 pieces.
 struct EvalDesc {
@@ -271,6 +289,7 @@ struct EvalDesc {
     u64 total;
 };
 
+#ifdef __CUDACC__
 __device__ __forceinline__ i64 piece_mcount(i64 lo, i64 hi) {
     return lo > hi ? 0 : hi / 6 - lo / 6 + 1;
 }
@@ -444,5 +463,7 @@ __device__ __forceinline__ u64 warp_sum_u64(u64 v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
+
+#endif  // __CUDACC__
 
 }  // namespace drb

@@ -1,4 +1,4 @@
-// dr_engine.cu -- host side of the B200 Deleglise-Rivat engine and its C ABI.
+// dr_engine.cpp -- host side (C++20) of the B200 Deleglise-Rivat engine and its C ABI.
 //
 // One dr_ctx owns a CUDA stream and grow-only device buffers.  A query runs as
 //   table build : sieve_kernel -> seg_scan_kernel -> fixup_kernel

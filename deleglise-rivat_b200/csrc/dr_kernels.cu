@@ -277,6 +277,27 @@ __device__ __forceinline__ void mark_item_from(uint32_t* buf32, const uint4 I, u
 }
 
 
+// Weight w at bytes j, j + p, j + 2p, ... below nb (one thread, p odd).  Four
+// consecutive hits span 4p bytes = p words, so their byte positions within the word
+// repeat every four hits: the four shifted weights and word offsets are set up once
+// and each group of four hits is four atomics and one pointer step.
+__device__ __forceinline__ void mark_prime(uint32_t* buf32, uint32_t j, uint32_t p, uint32_t w, uint32_t nb) {
+    if (j + 4u * p <= nb) {  // at least four hits: the unrolled loop
+        const uint32_t j1 = j + p, j2 = j1 + p, j3 = j2 + p;
+        const uint32_t v0 = w << ((j & 3u) * 8u), v1 = w << ((j1 & 3u) * 8u);
+        const uint32_t v2 = w << ((j2 & 3u) * 8u), v3 = w << ((j3 & 3u) * 8u);
+        const uint32_t o1 = (j1 >> 2) - (j >> 2), o2 = (j2 >> 2) - (j >> 2), o3 = (j3 >> 2) - (j >> 2);
+        uint32_t* q = buf32 + (j >> 2);
+        for (; j + 3u * p < nb; j += 4u * p, q += p) {
+            atomicAdd(q, v0);
+            atomicAdd(q + o1, v1);
+            atomicAdd(q + o2, v2);
+            atomicAdd(q + o3, v3);
+        }
+    }
+    for (; j < nb; j += p) atomicAdd(&buf32[j >> 2], w << ((j & 3) * 8));
+}
+
 // Marks of one warp item I = {modulus m, first byte, weight or 0x80, prime index |
 // square bit 31}: lanes stride the multiples of m at or after byte I.y (ODD: the odd
 // multiples, m bytes apart), 32 strides each, with the 64-bit reciprocal inv of m.
@@ -468,8 +489,7 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
                 r = (uint32_t)umod_inv((u64)low, p, a.pinv[i]);
             uint32_t d = r ? p - r : 0;
             if (ODD && (d & 1u)) d += p;
-            for (uint32_t j = ODD ? d >> 1 : d; j < (uint32_t)nb; j += p)
-                atomicAdd(&buf32[j >> 2], w << ((j & 3) * 8));
+            mark_prime(buf32, ODD ? d >> 1 : d, p, w, (uint32_t)nb);
             i = inext;
         }
         __syncthreads();

@@ -17,7 +17,7 @@ SRC = os.path.join(ROOT, "tests", "cpp", "shim_kat.cpp")
 def _build(tmp_path):
     libdir = os.path.dirname(dr_b200.build_library())
     exe = str(tmp_path / "shim_kat")
-    cmd = ["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), SRC, "-o", exe,
+    cmd = ["g++", "-std=c++20", "-O2", "-I", os.path.join(ROOT, "include"), SRC, "-o", exe,
            "-L", libdir, "-ldrb200", f"-Wl,-rpath,{libdir}"]
     subprocess.run(cmd, check=True)
     return exe
