@@ -254,33 +254,28 @@ __device__ __forceinline__ void planes_odd_mode(const SieveArgs& a, const uint32
     *neg = g;
 }
 
-// Marks of one warp item I from its first hit at byte j0: the item's multiples
-// k = 0 .. 1023 (byte j0 + k*m, below the end of the sieved bytes) are dealt as
-// k = 4l + phi + 128t to lane l, phase phi < 4, stride t < 8.  In one instruction
-// (phi, t fixed) the 32 lanes' bytes are C + 4*l*m: one byte position within the
-// word for all lanes (one shifted mark per phase) and words ~C/4 + l*m, which for
-// odd m fall on 32 distinct banks -- the shared-memory atomics never conflict.  A
-// lane's next hit of a phase is 128*m bytes = 32*m words further.
+// Marks of one warp item I from its first hit at byte j0 (lane l takes j0 + l*m, then
+// every 32nd multiple, up to the item's 1024 hits or the end of the sieved bytes).
+// A lane's strides are 32*m bytes, a multiple of 4: its byte position within the
+// 32-bit word, and so the shifted mark, stays the same, and the word advances by 8*m.
 __device__ __forceinline__ void mark_item_from(uint32_t* buf32, const uint4 I, uint32_t j0, int nb, int lane) {
     const uint32_t m = I.x;
+    const uint32_t j = j0 + (uint32_t)lane * m;
     const uint32_t jend = min((uint32_t)nb, I.y + 1024u * m);
-    const uint32_t w = (I.w >> 31) ? 0x80u : I.z;
-    const bool flag = I.w >> 31;
-#pragma unroll
-    for (uint32_t phi = 0; phi < 4u; ++phi) {
-        const uint32_t j = j0 + (4u * (uint32_t)lane + phi) * m;
-        const uint32_t ph = j & 3u;
-        // byte 4*(p - buf32) + ph < jend  <=>  p - buf32 < (jend - ph + 3) / 4
-        uint32_t* p = buf32 + (j >> 2);
-        uint32_t* const pend = buf32 + ((jend + 3u - ph) >> 2);
-        const uint32_t v = w << (8u * ph);
-        if (flag) {
-            for (; p < pend; p += 32u * m) atomicOr(p, v);
-        } else {
-            for (; p < pend; p += 32u * m) atomicAdd(p, v);
-        }
+    const uint32_t ph = j & 3u;
+    // byte 4*(p - buf32) + ph < jend  <=>  p - buf32 < (jend - ph + 3) / 4
+    const uint32_t wend = jend + 3u >= ph ? (jend + 3u - ph) >> 2 : 0u;
+    uint32_t* p = buf32 + (j >> 2);
+    uint32_t* const pend = buf32 + wend;
+    if (I.w >> 31) {
+        const uint32_t v = 0x80u << (8u * ph);
+        for (; p < pend; p += 8u * m) atomicOr(p, v);
+    } else {
+        const uint32_t v = I.z << (8u * ph);
+        for (; p < pend; p += 8u * m) atomicAdd(p, v);
     }
 }
+
 
 // Weight w at bytes j, j + p, j + 2p, ... below nb (one thread, p odd).  Four
 // consecutive hits span 4p bytes = p words, so their byte positions within the word
