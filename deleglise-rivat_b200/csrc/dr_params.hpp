@@ -180,18 +180,19 @@ inline void ref_gpu_params(int64_t X, int threads, dr_params* p) {
 }
 
 // B200 policy (DR_POLICY_GPU), fitted to sweeps of measured device times over
-// X = 10^14 .. 10^18 (fx in 0.15 .. 1.3, cx in 1 .. 2.1; table build ~1.3 ms per
-// 10^9 values with the odd-value sieve, S1 ~1.2 ms per 10^9 lookups, S2 ~1.9 ms
-// per 10^9 wheel positions): the table is far cheaper to build on the GPU than on
-// the CPU, so u is raised to 0.9 (X / ln ln X)^(2/3) -- the reference's u formula
-// without its 8e9 cap -- and cx = 1.3 (the optimum is flat: fx 0.75 .. 1.1 within
-// 1.5% at X = 10^16).  u is capped at 2.5e11 values (~80 GB of compressed tier) and
+// X = 10^14 .. 10^18 (table build ~1.0 ms per 10^9 values with the odd-value sieve,
+// S1 ~1.1 ms per 10^9 lookups, S2 ~1.9 ms per 10^9 wheel positions): the table is far
+// cheaper to build on the GPU than on the CPU, so u is raised to
+// 1.15 (X / ln ln X)^(2/3) -- the reference's u formula without its 8e9 cap -- and
+// cx = 1.25.  The optimum is flat: at X = 10^16 every (cx, fx) in [1.2, 1.3] x
+// [1.1, 1.35] is within 1% of the best, at 10^17 every cx in [1.2, 1.3] with
+// fx = 1.1 .. 1.3.  u is capped at 2.5e11 values (~80 GB of compressed tier) and
 // never below the endpoints; the dense tier holds max(1.28e8, u/16) values (<= 4e9).
 inline void gpu_params(int64_t X, dr_params* p) {
     params_clear(p);
-    const double cx = 1.3;
+    const double cx = 1.25;
     const double loglogX = std::log(std::max(2.0, std::log((double)X)));
-    int64_t u = (int64_t)(0.9 * std::pow((double)X / loglogX, 2.0 / 3.0));
+    int64_t u = (int64_t)(1.15 * std::pow((double)X / loglogX, 2.0 / 3.0));
     const int64_t S = isqrt_i64(X);
     u = std::max(u, 3 * S);
     u = std::min<int64_t>(u, 250000000000LL);
