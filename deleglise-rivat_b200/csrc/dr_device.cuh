@@ -289,6 +289,18 @@ struct EvalDesc {
     u64 total;
 };
 
+// One evaluation slot as the planner leaves it for the sums kernel (96 bytes): y, the
+// split points, the S1 segments and, in `bits`, the kind (bits 0-1), the sign of the
+// coefficient (bit 2) and per S1 segment g a stride code and sign (bits 3+3g ..).
+struct __align__(16) SlotDesc {
+    u64 y;
+    i64 A, B;
+    i64 n0[kS1Seg];
+    i64 cnt[kS1Seg];
+    u64 bits;
+};
+static_assert(sizeof(SlotDesc) == 96, "SlotDesc is six 16-byte words");
+
 #ifdef __CUDACC__
 __device__ __forceinline__ i64 piece_mcount(i64 lo, i64 hi) {
     return lo > hi ? 0 : hi / 6 - lo / 6 + 1;
@@ -310,6 +322,46 @@ __device__ __forceinline__ void s1_set(EvalDesc& d, int g, i64 n0, int stride, i
     d.s1_sign[g] = sign;
     if (stride == S1_WHEEL) d.s1_cnt[g] = last >= 0 && last >= n0 ? last - n0 + 1 : 0;  // n0, last: wheel indices
     else d.s1_cnt[g] = last >= n0 ? (last - n0) / stride + 1 : 0;
+}
+
+// The S2 pieces of an evaluation from its kind and split points (A; B = the split
+// point of y/2 for comb2): single pieces 9..12 over j in [1, A/6], (A/6, A/3],
+// (A/3, A/2], (A/2, A]; combined pieces 1..8 cut at B/6 A/6 B/3 A/3 B/2 A/2 B A
+// (eval_s2_single / eval_s2_combined, mertens_dr.hpp:622-660).
+__device__ __forceinline__ void eval_pieces(EvalDesc& d) {
+    const i64 A = d.A, B = d.B;
+    if (d.kind == EVAL_SINGLE) {
+        d.npieces = 4; d.piece0 = 9;
+        const i64 a6 = A / 6, a3 = A / 3, a2 = A / 2;
+        d.jlo[0] = 1;      d.jhi[0] = a6;
+        d.jlo[1] = a6 + 1; d.jhi[1] = a3;
+        d.jlo[2] = a3 + 1; d.jhi[2] = a2;
+        d.jlo[3] = a2 + 1; d.jhi[3] = A;
+    } else {
+        d.npieces = 8; d.piece0 = 1;
+        const i64 b6 = B / 6, a6 = A / 6, b3 = B / 3, a3 = A / 3, b2 = B / 2, a2 = A / 2;
+        d.jlo[0] = 1;      d.jhi[0] = b6;
+        d.jlo[1] = b6 + 1; d.jhi[1] = a6;
+        d.jlo[2] = a6 + 1; d.jhi[2] = b3;
+        d.jlo[3] = b3 + 1; d.jhi[3] = a3;
+        d.jlo[4] = a3 + 1; d.jhi[4] = b2;
+        d.jlo[5] = b2 + 1; d.jhi[5] = a2;
+        d.jlo[6] = a2 + 1; d.jhi[6] = B;
+        d.jlo[7] = B + 1;  d.jhi[7] = A;
+    }
+    d.nseg = kS1Seg + d.npieces;
+}
+
+// Wheel positions of every piece and the evaluation's op count (S1 lookups left to
+// the sums kernel + S2 wheel positions).
+__device__ __forceinline__ void eval_total(EvalDesc& d) {
+    u64 tot = 0;
+    for (int g = 0; g < kS1Seg; ++g) tot += (u64)d.s1_cnt[g];
+    for (int p = 0; p < d.npieces; ++p) {
+        d.mcnt[p] = piece_mcount(d.jlo[p], d.jhi[p]);
+        tot += (u64)d.mcnt[p];
+    }
+    d.total = tot;
 }
 
 // Decode evaluation e (0/1) of candidate c of query Q.  Follows the outer
@@ -377,12 +429,7 @@ __device__ inline void decode_eval(const QueryDev& Q, const TableView& T, i64 c,
         } else {
             s1_set(d, 0, start, 1, ky, 1);
         }
-        d.npieces = 4; d.piece0 = 9;
-        const i64 a6 = A / 6, a3 = A / 3, a2 = A / 2;
-        d.jlo[0] = 1;      d.jhi[0] = a6;
-        d.jlo[1] = a6 + 1; d.jhi[1] = a3;
-        d.jlo[2] = a3 + 1; d.jhi[2] = a2;
-        d.jlo[3] = a2 + 1; d.jhi[3] = A;
+        eval_pieces(d);
     } else {
         const i64 A = split_point(Q.cx, (i64)y);
         const i64 B = split_point(Q.cx, (i64)y2);
@@ -411,18 +458,8 @@ __device__ inline void decode_eval(const QueryDev& Q, const TableView& T, i64 c,
         else if (two < ky) { e0 = two + 1; last = ky; sg = 1; }
         if (e0 & 1) ++e0;
         s1_set(d, 3, e0, 2, last, sg);
-        d.npieces = 8; d.piece0 = 1;
-        const i64 b6 = B / 6, a6 = A / 6, b3 = B / 3, a3 = A / 3, b2 = B / 2, a2 = A / 2;
-        d.jlo[0] = 1;      d.jhi[0] = b6;
-        d.jlo[1] = b6 + 1; d.jhi[1] = a6;
-        d.jlo[2] = a6 + 1; d.jhi[2] = b3;
-        d.jlo[3] = b3 + 1; d.jhi[3] = a3;
-        d.jlo[4] = a3 + 1; d.jhi[4] = b2;
-        d.jlo[5] = b2 + 1; d.jhi[5] = a2;
-        d.jlo[6] = a2 + 1; d.jhi[6] = B;
-        d.jlo[7] = B + 1;  d.jhi[7] = A;
+        eval_pieces(d);
     }
-    d.nseg = kS1Seg + d.npieces;
     // windowed S1: the lookups with q < wc*W, i.e. n > y/(wc*W), go to s1win_kernel
     for (int g = 0; g < kS1Seg; ++g) {
         d.s1_full[g] = d.s1_cnt[g];
@@ -440,13 +477,59 @@ __device__ inline void decode_eval(const QueryDev& Q, const TableView& T, i64 c,
         if (st == S1_WHEEL) d.s1_cnt[g] = min(cnt, max(0ll, wheel_upper(ncut - 1) - d.s1_n0[g] + 1));
         else d.s1_cnt[g] = ncut <= d.s1_n0[g] ? 0 : min(cnt, (ncut - 1 - d.s1_n0[g]) / st + 1);
     }
-    u64 tot = 0;
-    for (int g = 0; g < kS1Seg; ++g) tot += (u64)d.s1_cnt[g];
-    for (int p = 0; p < d.npieces; ++p) {
-        d.mcnt[p] = piece_mcount(d.jlo[p], d.jhi[p]);
-        tot += (u64)d.mcnt[p];
+    eval_total(d);
+}
+
+// Stride codes of SlotDesc: 1, 2, 6 and the wheel (S1_WHEEL) in two bits.
+__device__ __forceinline__ u64 stride_code(int st) { return st == 1 ? 0u : st == 2 ? 1u : st == 6 ? 2u : 3u; }
+__device__ __forceinline__ int stride_of_code(u64 c) { return c == 0 ? 1 : c == 1 ? 2 : c == 2 ? 6 : S1_WHEEL; }
+
+// An evaluation as the sums kernel needs it, written once by the planner.
+__device__ __forceinline__ void pack_slot(const EvalDesc& d, SlotDesc* out) {
+    SlotDesc s;
+    if (d.kind == EVAL_NONE) {  // no terms: the sums kernel never reads it
+        s.y = 0;
+        s.A = s.B = 0;
+        for (int g = 0; g < kS1Seg; ++g) s.n0[g] = s.cnt[g] = 0;
+        s.bits = 0;
+        *out = s;
+        return;
     }
-    d.total = tot;
+    s.y = d.y;
+    s.A = d.A;
+    s.B = d.kind == EVAL_COMB2 ? d.B : 0;
+    u64 bits = (u64)d.kind | (d.coef < 0 ? 4ull : 0ull);
+    for (int g = 0; g < kS1Seg; ++g) {
+        s.n0[g] = d.s1_n0[g];
+        s.cnt[g] = d.s1_cnt[g];
+        bits |= (stride_code(d.s1_stride[g]) | (d.s1_sign[g] < 0 ? 4ull : 0ull)) << (3 + 3 * g);
+    }
+    s.bits = bits;
+    *out = s;
+}
+
+// The planner's evaluation back from its SlotDesc: S1 segments as stored, S2
+// pieces and op count recomputed from the split points.
+__device__ __forceinline__ void unpack_slot(const SlotDesc& s, EvalDesc& d) {
+    d.y = s.y;
+    d.kind = (int)(s.bits & 3u);
+    d.coef = (s.bits & 4u) ? -1 : 1;
+    d.A = s.A;
+    d.B = s.B;
+    for (int g = 0; g < kS1Seg; ++g) {
+        const u64 c = s.bits >> (3 + 3 * g);
+        d.s1_n0[g] = s.n0[g];
+        d.s1_cnt[g] = s.cnt[g];
+        d.s1_stride[g] = stride_of_code(c & 3u);
+        d.s1_sign[g] = (c & 4u) ? -1 : 1;
+    }
+    if (d.kind == EVAL_NONE) {
+        d.nseg = 0;
+        d.total = 0;
+        return;
+    }
+    eval_pieces(d);
+    eval_total(d);
 }
 
 // Constant part of an evaluation: 1 + kappa*M(A) (single) or

@@ -72,7 +72,7 @@ struct dr_ctx {
     DevBuf items_odd, stencil_odd, dplanes;  // odd-mode sieve: items, stencil, dense-tier plane words
     DevBuf sq_cnt, sq_off, sq_cur, sq_pos, sq_tmp;  // bucketed square hits per segment
     // query buffers
-    DevBuf queries, ops, prefix, scan_tmp, acc, counts, ticket, misc, inv, invw, wdesc, witems;
+    DevBuf queries, ops, prefix, scan_tmp, acc, counts, ticket, misc, inv, invw, wdesc, witems, slots;
     // table state
     bool table_valid = false;
     int64_t t_u_total = 0, t_u_dense = 0, t_mu_limit = 0, t_nwords = 0;
@@ -601,6 +601,7 @@ int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq,
     if ((rc = ensure(c, c->counts, (size_t)nq * kCountsPerQuery * 8))) return rc;
     if ((rc = ensure(c, c->ops, (size_t)std::max<u64>(slots, 1) * 8))) return rc;
     if ((rc = ensure(c, c->prefix, (size_t)(slots + 1) * 8))) return rc;
+    if ((rc = ensure(c, c->slots, (size_t)std::max<u64>(slots, 1) * sizeof(SlotDesc)))) return rc;
     if ((rc = ensure(c, c->scan_tmp, scan_u64_tmp_elems(slots) * 8))) return rc;
     if ((rc = ensure(c, c->ticket, 32))) return rc;
     if (!witems.empty()) {
@@ -651,7 +652,7 @@ int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq,
         launch_inverse((double*)c->inv.p, inv_limit, (double2*)c->invw.p, invw_count, T.wheel, c->sm_count,
                        c->stream);
         launch_plan((const QueryDev*)c->queries.p, qn, T, slots, (u64*)c->ops.p, (u64*)c->acc.p, (i64*)c->counts.p,
-                    sw ? (S1WinDesc*)c->wdesc.p : nullptr, c->sm_count, c->stream);
+                    sw ? (S1WinDesc*)c->wdesc.p : nullptr, (SlotDesc*)c->slots.p, c->sm_count, c->stream);
         launch_scan_u64((const u64*)c->ops.p, (u64*)c->prefix.p, slots, (u64*)c->scan_tmp.p,
                         scan_u64_tmp_elems(slots), c->stream);
         launches += 5;
@@ -679,6 +680,7 @@ int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq,
         sa.T = T;
         sa.n_slots = slots;
         sa.prefix = (const u64*)c->prefix.p;
+        sa.slots = (const SlotDesc*)c->slots.p;
         sa.ticket = (u64*)c->ticket.p;
         sa.acc = (u64*)c->acc.p;
         sa.chunk_log2 = tuning ? tuning->chunk_log2 : 0;
@@ -874,7 +876,7 @@ int dr_ctx_destroy(dr_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     DevBuf* bufs[] = {&c->dM, &c->planes, &c->ckpt, &c->wheel, &c->seg_sum, &c->seg_off, &c->primes, &c->pinv, &c->items, &c->stencil,
                       &c->queries, &c->ops, &c->prefix, &c->scan_tmp, &c->acc, &c->counts, &c->ticket, &c->misc,
-                      &c->inv, &c->invw, &c->wdesc, &c->witems, &c->prcp, &c->sq_cnt, &c->sq_off, &c->sq_cur,
+                      &c->inv, &c->invw, &c->wdesc, &c->witems, &c->slots, &c->prcp, &c->sq_cnt, &c->sq_off, &c->sq_cur,
                       &c->sq_pos, &c->sq_tmp, &c->items_odd, &c->stencil_odd, &c->dplanes};
     for (DevBuf* b : bufs) release(c, *b);
     drop_graphs(c);
@@ -953,7 +955,7 @@ uint64_t dr_query_bytes(int64_t X, const dr_params* p) {
     if (X > p->u_total && p->cx > 0.0) {
         const double inv = 1.4143 * std::sqrt((double)X) / p->cx + 65.0;  // S1 reciprocals
         const int64_t slots = 2 * num_candidates(X / p->u_total);        // ops + prefix
-        b += (uint64_t)(8.0 * inv) + (uint64_t)(p->mu_limit / 6 + 1) * 16 + (uint64_t)slots * 16 +
+        b += (uint64_t)(8.0 * inv) + (uint64_t)(p->mu_limit / 6 + 1) * 16 + (uint64_t)slots * (16 + sizeof(SlotDesc)) +
              scan_u64_tmp_elems((u64)slots) * 8;
     }
     return b;

@@ -958,7 +958,7 @@ __device__ __forceinline__ u64 s1_compressed_lookups(const EvalDesc& d, const Ta
 // positions, compressed-tier S1 lookups -- summed over the warp before the atomics
 __global__ void plan_kernel(const QueryDev* __restrict__ qs, int nq, const TableView T, u64 n_slots,
                             u64* __restrict__ ops, u64* __restrict__ acc, i64* __restrict__ counts,
-                            S1WinDesc* __restrict__ wdesc) {
+                            S1WinDesc* __restrict__ wdesc, SlotDesc* __restrict__ slots) {
     // whole warps step together (the stride is a multiple of 32), so the counters
     // can be summed over the warp with every lane taking part
     const u64 stride = (u64)gridDim.x * blockDim.x;
@@ -974,6 +974,7 @@ __global__ void plan_kernel(const QueryDev* __restrict__ qs, int nq, const Table
             EvalDesc d;
             decode_eval(Q, T, (i64)(local >> 1), (int)(local & 1), d);
             ops[s] = d.total;
+            pack_slot(d, slots + s);
             if (wdesc && Q.win) {
                 S1WinDesc w;
                 w.y = d.y;
@@ -1024,10 +1025,10 @@ __global__ void plan_kernel(const QueryDev* __restrict__ qs, int nq, const Table
 }
 
 void launch_plan(const QueryDev* q, int nq, const TableView& T, u64 n_slots, u64* ops, u64* acc, i64* counts,
-                 S1WinDesc* wdesc, int sm_count, cudaStream_t s) {
+                 S1WinDesc* wdesc, SlotDesc* slots, int sm_count, cudaStream_t s) {
     if (n_slots == 0) return;
     const int grid = (int)std::min<u64>((n_slots + 127) / 128, (u64)sm_count * 16);
-    plan_kernel<<<grid, 128, 0, s>>>(q, nq, T, n_slots, ops, acc, counts, wdesc);
+    plan_kernel<<<grid, 128, 0, s>>>(q, nq, T, n_slots, ops, acc, counts, wdesc, slots);
 }
 
 // Direct answers for queries with X <= table u_total (get_M, :1465-1467).
@@ -1457,11 +1458,7 @@ __global__ void __launch_bounds__(256, DRB_SUMS_MINB) sums_kernel(const SumsArgs
             const u64 sbase = a.prefix[s];
             const int qi = a.nq == 1 ? 0 : query_of_slot(a.queries, a.nq, s);
             __syncwarp();
-            if (lane == 0) {
-                const QueryDev Q = a.queries[qi];
-                const u64 local = s - Q.slot_base;
-                decode_eval(Q, a.T, (i64)(local >> 1), (int)(local & 1), d);
-            }
+            if (lane == 0) unpack_slot(a.slots[s], d);  // the planner's decoded evaluation
             __syncwarp();
             if (qi != cur_q) {
                 if (cur_q >= 0) {

@@ -91,6 +91,7 @@ struct SumsArgs {
     TableView T;
     u64 n_slots;
     const u64* prefix;  // [n_slots + 1] exclusive op prefix
+    const SlotDesc* slots;  // [n_slots] each slot's evaluation, written by plan_kernel
     u64* ticket;        // [0]: work-queue counter, [1]: error flag; zeroed before launch
     u64* acc;           // [3 * nq]: C, S1, S2
     int chunk_log2;     // 0: chosen on the device from the total
@@ -131,7 +132,7 @@ void launch_fixup(int16_t* dM, i64 u_dense, int S, const int32_t* seg_off, int32
 // whose quotient lies in the compressed tier (q > u_dense).
 constexpr int kCountsPerQuery = 5;
 void launch_plan(const QueryDev* q, int nq, const TableView& T, u64 n_slots, u64* ops, u64* acc,
-                 i64* counts, S1WinDesc* wdesc, int sm_count, cudaStream_t s);
+                 i64* counts, S1WinDesc* wdesc, SlotDesc* slots, int sm_count, cudaStream_t s);
 // Windowed S1 (window length win: a power of two, 2^12 .. 2^16).
 void launch_s1win(const S1WinArgs& a, u64 win, int sm_count, cudaStream_t s);
 void launch_scan_u64(const u64* in, u64* out, u64 n, u64* tmp, size_t tmp_elems, cudaStream_t s);
