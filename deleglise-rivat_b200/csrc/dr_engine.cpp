@@ -86,6 +86,12 @@ struct dr_ctx {
     size_t pinned_cap = 0;
     std::vector<uint64_t> last_sums;
     cudaEvent_t ev[8] = {};
+    // side stream of the table build: the segment scan and fix-up of each finished
+    // sieve launch run there, beside the next sieve launch (fork/join by events)
+    cudaStream_t side = nullptr;
+    static constexpr int kForks = 40;
+    cudaEvent_t fork[kForks] = {};
+    cudaEvent_t join = nullptr;
     bool sieve_attr_set = false;
     // pinned staging for every host->device source of a call (a captured graph
     // owns its own staging, so replays never read memory a later call reuses)
@@ -291,7 +297,7 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     if ((rc = ensure(c, c->ckpt, (size_t)nwords * 4))) return rc;
     if ((rc = ensure(c, c->wheel, (size_t)wheel_groups * 16))) return rc;
     if ((rc = ensure(c, c->seg_sum, (size_t)nseg * 4))) return rc;
-    if ((rc = ensure(c, c->seg_off, (size_t)nseg * 4))) return rc;
+    if ((rc = ensure(c, c->seg_off, (size_t)(nseg + 1) * 4))) return rc;
     const std::vector<uint32_t>& pr = primes_upto(c, isqrt_i64(u_total));
     if ((rc = ensure(c, c->primes, pr.size() * 4))) return rc;
     if ((rc = ensure(c, c->pinv, pr.size() * 16))) return rc;
@@ -412,20 +418,37 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
         CU(cudaGetLastError());
         launches += 5;
     }
-    for (const SieveLaunch& l : plan) {
+    // Each sieve launch covers the segments [begin, end) in order.  Once it is done, the
+    // side stream scans their Mobius sums (continuing from the segments before) and
+    // adds the offsets to their dense prefix values and checkpoints, while the main
+    // stream sieves the next range: the fix-up, a pure memory pass, runs beside the
+    // integer-bound sieve.  Nothing the sieve reads (plane words) is written by it.
+    // More launches than fork events (never expected): the rest fix up at the end.
+    int forks = 0;
+    int64_t fixed = 0;  // segments below it are scanned and fixed up on the side stream
+    for (size_t li = 0; li < plan.size(); ++li) {
+        const SieveLaunch& l = plan[li];
         SieveArgs& m = l.odd ? ao : a;
         m.seg_begin = l.begin;
         m.seg_end = l.end;
         launch_sieve(m, l.odd, (int)std::max<int64_t>(1, std::min<int64_t>(l.end - l.begin, l.odd ? grid_o : grid_f)),
                      block, l.odd ? smem_o : smem_f, c->stream);
         CU(cudaGetLastError());
+        if (forks < dr_ctx::kForks - 1 || li + 1 == plan.size()) {
+            CU(cudaEventRecord(c->fork[forks], c->stream));
+            CU(cudaStreamWaitEvent(c->side, c->fork[forks], 0));
+            launch_seg_scan_range((const int32_t*)c->seg_sum.p, (int32_t*)c->seg_off.p, fixed, l.end, c->side);
+            launch_fixup_range((int16_t*)c->dM.p, u_dense, S, (const int32_t*)c->seg_off.p, (int32_t*)c->ckpt.p,
+                               nwords, dense_segs, fixed, l.end, c->sm_count * 2, c->side);
+            CU(cudaGetLastError());
+            fixed = l.end;
+            ++forks;
+            launches += 2;
+        }
     }
-    launches += (int)plan.size() - 1;
-    launch_seg_scan((const int32_t*)c->seg_sum.p, (int32_t*)c->seg_off.p, nseg, c->stream);
-    CU(cudaGetLastError());
-    launch_fixup((int16_t*)c->dM.p, u_dense, S, (const int32_t*)c->seg_off.p, (int32_t*)c->ckpt.p, nwords,
-                 dense_segs, c->sm_count, c->stream);
-    CU(cudaGetLastError());
+    CU(cudaEventRecord(c->join, c->side));
+    CU(cudaStreamWaitEvent(c->stream, c->join, 0));
+    launches += (int)plan.size() - 3;
     CU(record_event(c, 1));
 
     c->table_valid = true;
@@ -850,6 +873,13 @@ int dr_ctx_create(int device, void* cuda_stream, dr_ctx** out) {
     cudaMemGetInfo(&free_b, &total_b);
     c->budget = (uint64_t)((double)free_b * 0.92);
     for (auto& e : c->ev) cudaEventCreate(&e);
+    for (auto& e : c->fork) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming);
+    if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess) {
+        c->side = nullptr;
+        dr_ctx_destroy(c);
+        return fail(DR_ERR_CUDA, "cudaStreamCreate (side stream) failed");
+    }
     init_piece_constants();
     std::vector<uint32_t> st = make_stencil4();
     std::vector<uint32_t> sto = make_stencil_odd4();
@@ -885,6 +915,13 @@ int dr_ctx_destroy(dr_ctx* c) {
     if (c->wstage) cudaFreeHost(c->wstage);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
+    if (c->side) {
+        cudaStreamSynchronize(c->side);
+        cudaStreamDestroy(c->side);
+    }
+    for (auto& e : c->fork)
+        if (e) cudaEventDestroy(e);
+    if (c->join) cudaEventDestroy(c->join);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return DR_OK;

@@ -872,31 +872,41 @@ void launch_sq_bucket_fill(const uint32_t* primes, int first, int n, i64 u_total
 // ---------------------------------------------------------------------------
 // Segment offsets (single block) and the fix-up pass.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) seg_scan_kernel(const int32_t* in, int32_t* out, i64 n) {
+// out[i] = sum of in[j] for j < i, for i in [b0, b1], given out[b0] (0 for b0 = 0):
+// the segment offsets of the segments [b0, b1) plus the running total at b1, so that
+// the scan of the next range [b1, ...) can start there.
+__global__ void __launch_bounds__(1024) seg_scan_kernel(const int32_t* in, int32_t* out, i64 b0, i64 b1) {
     __shared__ int32_t tile[1024];
     __shared__ int32_t wtot[33];
-    int carry = 0;
-    for (i64 b = 0; b < n; b += 1024) {
+    int carry = b0 == 0 ? 0 : out[b0];
+    for (i64 b = b0; b < b1; b += blockDim.x) {
         const i64 i = b + threadIdx.x;
-        tile[threadIdx.x] = i < n ? in[i] : 0;
+        tile[threadIdx.x] = i < b1 ? in[i] : 0;
         __syncthreads();
-        const int tot = block_excl_scan(tile, 1024, wtot);
-        if (i < n) out[i] = carry + tile[threadIdx.x];
+        const int tot = block_excl_scan(tile, (int)blockDim.x, wtot);
+        if (i < b1) out[i] = carry + tile[threadIdx.x];
         carry += tot;
         __syncthreads();
     }
+    if (threadIdx.x == 0) out[b1] = carry;
 }
 
 void launch_seg_scan(const int32_t* in, int32_t* out, i64 n, cudaStream_t s) {
-    seg_scan_kernel<<<1, 1024, 0, s>>>(in, out, n);
+    seg_scan_kernel<<<1, 1024, 0, s>>>(in, out, 0, n);
 }
 
-__global__ void fixup_kernel(int16_t* dM, i64 u_dense, int lgS, const int32_t* seg_off, int32_t* ckpt, i64 nwords,
-                             i64 dense_segs) {
+void launch_seg_scan_range(const int32_t* in, int32_t* out, i64 b0, i64 b1, cudaStream_t s) {
+    if (b1 > b0) seg_scan_kernel<<<1, 256, 0, s>>>(in, out, b0, b1);
+}
+
+// Adds the segment offsets to the dense prefix values of the 8-value groups [g0, g1)
+// and to the checkpoints [w0, w1) (int16 wrap-around on the dense tier, as the
+// reference's int16 conversion).
+__global__ void fixup_kernel(int16_t* dM, i64 u_dense, int lgS, const int32_t* seg_off, int32_t* ckpt, i64 g0,
+                             i64 g1, i64 w0, i64 w1, i64 dense_segs) {
     const i64 stride = (i64)gridDim.x * blockDim.x;
     const i64 t0 = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    const i64 n8 = (u_dense + 7) / 8;
-    for (i64 i = t0; i < n8; i += stride) {
+    for (i64 i = g0 + t0; i < g1; i += stride) {
         const int32_t off = seg_off[(8 * i) >> lgS];
         if (8 * i + 8 <= u_dense) {
             uint4* p = reinterpret_cast<uint4*>(dM) + i;
@@ -911,17 +921,31 @@ __global__ void fixup_kernel(int16_t* dM, i64 u_dense, int lgS, const int32_t* s
             for (i64 k = 8 * i; k < u_dense; ++k) dM[k] = (int16_t)(dM[k] + off);
         }
     }
-    for (i64 w = t0; w < nwords; w += stride) ckpt[w] += seg_off[dense_segs + ((64 * w) >> lgS)];
+    for (i64 w = w0 + t0; w < w1; w += stride) ckpt[w] += seg_off[dense_segs + ((64 * w) >> lgS)];
+}
+
+// The fix-up of segments [b0, b1): their dense groups and their checkpoint words.
+void launch_fixup_range(int16_t* dM, i64 u_dense, int S, const int32_t* seg_off, int32_t* ckpt, i64 nwords,
+                        i64 dense_segs, i64 b0, i64 b1, int blocks, cudaStream_t s) {
+    int lgS = 0;  // S is a power of two (2^12 .. 2^18)
+    while ((1 << lgS) < S) ++lgS;
+    const i64 n8 = (u_dense + 7) / 8;
+    const i64 g0 = std::min(n8, (b0 * (i64)S) / 8), g1 = std::min(n8, (std::min(b1, dense_segs) * (i64)S) / 8);
+    const i64 c0 = std::max(b0, dense_segs) - dense_segs, c1 = std::max(b1, dense_segs) - dense_segs;
+    const i64 w0 = std::min(nwords, c0 * (i64)(S / 64)), w1 = std::min(nwords, c1 * (i64)(S / 64));
+    // the last dense segment may end inside a group: its tail group belongs to it
+    const i64 g1x = (b1 >= dense_segs) ? n8 : g1;
+    const i64 work = std::max(g1x - g0, w1 - w0);
+    if (work <= 0) return;
+    const int grid = (int)std::max<i64>(1, std::min<i64>((work + 255) / 256, (i64)blocks));
+    fixup_kernel<<<grid, 256, 0, s>>>(dM, u_dense, lgS, seg_off, ckpt, g0, g1x, w0, w1, dense_segs);
 }
 
 void launch_fixup(int16_t* dM, i64 u_dense, int S, const int32_t* seg_off, int32_t* ckpt, i64 nwords,
                   i64 dense_segs, int sm_count, cudaStream_t s) {
-    const i64 work = max((u_dense + 7) / 8, nwords);
-    if (work <= 0) return;
-    int lgS = 0;  // S is a power of two (2^12 .. 2^18)
-    while ((1 << lgS) < S) ++lgS;
-    const int grid = (int)std::min<i64>((work + 255) / 256, (i64)sm_count * 8);
-    fixup_kernel<<<grid, 256, 0, s>>>(dM, u_dense, lgS, seg_off, ckpt, nwords, dense_segs);
+    const i64 nseg_all = dense_segs + (nwords * 64 + S - 1) / S;
+    launch_fixup_range(dM, u_dense, S, seg_off, ckpt, nwords, dense_segs, 0, std::max<i64>(nseg_all, dense_segs),
+                       sm_count * 8, s);
 }
 
 // ---------------------------------------------------------------------------
