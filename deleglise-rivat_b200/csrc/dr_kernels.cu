@@ -1192,7 +1192,23 @@ __device__ __forceinline__ double u32_to_double(uint32_t v) {
 // bound by it.
 __device__ __forceinline__ void rcp_group(const double* rcp, uint32_t nfirst, uint32_t nstep, double nstep_d,
                                           double* rv) {
-    if (nfirst >= 256u * nstep) {
+    if (nfirst >= 512u * nstep) {
+        // Second-order Taylor value r0*(1 - k*t + k^2*t^2), t = nstep*r0: relative error
+        // (k*t)^3 <= (7/512)^3 = 2^-18.5; one Newton step squares it to below 2^-37,
+        // still far inside the 32-bit route's need (q < 2^32: error below 2^-5)
+        const double r0 = __ldg(rcp + nfirst);
+        const double xr = nstep_d * r0 * r0;  // t * r0
+        const double x2 = xr * (nstep_d * r0);  // t^2 * r0
+        const double nd = u32_to_double(nfirst);
+        rv[0] = r0;
+#pragma unroll
+        for (int k = 1; k < kS1Unroll; ++k) {
+            const double nk = __fma_rn((double)k, nstep_d, nd);  // exact
+            double r = __fma_rn((double)(k * k), x2, __fma_rn(-(double)k, xr, r0));
+            r = __fma_rn(r, __fma_rn(-nk, r, 1.0), r);
+            rv[k] = r;
+        }
+    } else if (nfirst >= 256u * nstep) {
         const double r0 = __ldg(rcp + nfirst);
         const double xr = nstep_d * r0 * r0;
         const double nd = u32_to_double(nfirst);
