@@ -1164,10 +1164,11 @@ void launch_scan_u64(const u64* in, u64* out, u64 n, u64* tmp, size_t, cudaStrea
 // Persistent S1 / S2 kernel over the flattened op space.
 // ---------------------------------------------------------------------------
 
-// Code-shape knobs of the sums kernel (chosen by measurement on B200: 64
-// registers, 4 CTAs of 256 threads per SM).
+// Code-shape knobs of the sums kernel (chosen by measurement on B200: 80
+// registers, 3 CTAs of 256 threads per SM -- with the S1 software pipeline the
+// extra registers beat the fourth CTA: sums phase 49.3 against 50.2 ms at M(10^16)).
 #ifndef DRB_SUMS_MINB
-#define DRB_SUMS_MINB 4
+#define DRB_SUMS_MINB 3
 #endif
 #ifndef DRB_S1_UNROLL
 #define DRB_S1_UNROLL 8
@@ -1182,8 +1183,8 @@ __device__ __forceinline__ double u32_to_double(uint32_t v) {
 }
 
 // 1/n for the kS1Unroll divisors n = nfirst + nstep*k of a lane's group
-// (nfirst + nstep*(kS1Unroll-1) < 2^31).  From nfirst >= 256*nstep on, only 1/nfirst
-// is loaded; the others start from the first-order Taylor value r0*(1 -
+// (nfirst + nstep*(kS1Unroll-1) < 2^31), given r0 = 1/nfirst as tabulated.  From
+// nfirst >= 256*nstep on, only r0 is read; the others start from the first-order Taylor value r0*(1 -
 // k*nstep*r0), relative error (k*nstep/nfirst)^2 <= (7/256)^2 = 2^-10.4, and two Newton steps
 // r += r*(1 - n*r) square that error twice (to below 2^-41, on the FP64 pipe,
 // which the loop leaves idle) -- far inside what the 32-bit dense route needs
@@ -1191,12 +1192,11 @@ __device__ __forceinline__ double u32_to_double(uint32_t v) {
 // L2 traffic of the reciprocal table by a factor kS1Unroll where the loop is
 // bound by it.
 __device__ __forceinline__ void rcp_group(const double* rcp, uint32_t nfirst, uint32_t nstep, double nstep_d,
-                                          double* rv) {
+                                          const double r0, double* rv) {
     if (nfirst >= 512u * nstep) {
         // Second-order Taylor value r0*(1 - k*t + k^2*t^2), t = nstep*r0: relative error
         // (k*t)^3 <= (7/512)^3 = 2^-18.5; one Newton step squares it to below 2^-37,
         // still far inside the 32-bit route's need (q < 2^32: error below 2^-5)
-        const double r0 = __ldg(rcp + nfirst);
         const double xr = nstep_d * r0 * r0;  // t * r0
         const double x2 = xr * (nstep_d * r0);  // t^2 * r0
         const double nd = u32_to_double(nfirst);
@@ -1209,7 +1209,6 @@ __device__ __forceinline__ void rcp_group(const double* rcp, uint32_t nfirst, ui
             rv[k] = r;
         }
     } else if (nfirst >= 256u * nstep) {
-        const double r0 = __ldg(rcp + nfirst);
         const double xr = nstep_d * r0 * r0;
         const double nd = u32_to_double(nfirst);
         rv[0] = r0;
@@ -1223,14 +1222,19 @@ __device__ __forceinline__ void rcp_group(const double* rcp, uint32_t nfirst, ui
         }
     } else {
         const double* p = rcp + nfirst;
+        rv[0] = r0;
 #pragma unroll
-        for (int k = 0; k < kS1Unroll; ++k) rv[k] = __ldg(p + nstep * (uint32_t)k);
+        for (int k = 1; k < kS1Unroll; ++k) rv[k] = __ldg(p + nstep * (uint32_t)k);
     }
 }
 
 // sum of M(floor(y/n)) over n = n0 + stride*i, i in [i0, i1), lanes interleaved.
 // Each lane walks groups of kS1Unroll of its divisors (n, n + 32*stride, ...)
-// whose reciprocal loads, quotients and table gathers issue back to back.  A group
+// whose reciprocal loads, quotients and table gathers issue back to back, software
+// pipelined over the groups: a group's first reciprocal is loaded one group ahead,
+// and the gathers of a group on the dense route are summed one group later,
+// so a warp's reciprocal and table latencies overlap its own arithmetic instead of
+// adding up group after group.  A group
 // whose divisors are tabulated and below 2^31 and whose first (largest) quotient
 // is in the dense tier -- q falls as n grows, so then every quotient is -- runs on
 // 32-bit quotients (qest/qfix); the rest use the 64-bit routine (every q here is
@@ -1254,20 +1258,32 @@ __device__ __forceinline__ i64 s1_part(const SumsArgs& a, u64 y, i64 n0, int str
     const u64 gstep = (u64)nstep * kS1Unroll;
     const u64 nl = s1_n_at(n0, stride, il);  // this lane's first divisor
     u64 nfirst = nl;
+    int32_t pv[kS1Unroll];  // the previous dense group's gathered M values, not yet summed
+#pragma unroll
+    for (int k = 0; k < kS1Unroll; ++k) pv[k] = 0;
+    double r0 = groups && nl <= lim ? __ldg(a.rcp + nl) : 0.0;  // 1/nfirst of the coming group
     for (uint32_t g = 0; g < groups; ++g, nfirst += gstep) {
         const u64 nlast = nfirst + (u64)nstep * (kS1Unroll - 1);
+        const double r0g = r0;
+        r0 = g + 1 < groups && nfirst + gstep <= lim ? __ldg(a.rcp + nfirst + gstep) : 0.0;
         if (nlast <= lim31) {
             const uint32_t nf = (uint32_t)nfirst;
             double rv[kS1Unroll];
-            rcp_group(a.rcp, nf, nstep, nstep_d, rv);
+            rcp_group(a.rcp, nf, nstep, nstep_d, r0g, rv);
             // t0 = 2^52 + qest of the first divisor: qest <= u_dense bounds q
             const double t0 = __fma_ru(yd, rv[0], kQBias);
             if (t0 <= dense_t) {
-                int32_t part = 0;
+                uint32_t qq[kS1Unroll];
 #pragma unroll
                 for (int k = 0; k < kS1Unroll; ++k) {
                     const uint32_t qp = k == 0 ? (uint32_t)__double2loint(t0) : qest(yd, rv[k]);
-                    part += __ldg(dMm1 + qfix(qp, ylo, nf + nstep * (uint32_t)k));
+                    qq[k] = qfix(qp, ylo, nf + nstep * (uint32_t)k);
+                }
+                int32_t part = 0;
+#pragma unroll
+                for (int k = 0; k < kS1Unroll; ++k) {
+                    part += pv[k];
+                    pv[k] = __ldg(dMm1 + qq[k]);
                 }
                 acc += part;
             } else {  // compressed tier (rare): exact tabulated reciprocals for udiv_rcp
@@ -1284,6 +1300,12 @@ __device__ __forceinline__ i64 s1_part(const SumsArgs& a, u64 y, i64 n0, int str
                 acc += table_M(a.T, n <= lim ? udiv_rcp(y, yd, (uint32_t)n, __ldg(a.rcp + n)) : udiv(y, n));
             }
         }
+    }
+    {
+        int32_t part = 0;
+#pragma unroll
+        for (int k = 0; k < kS1Unroll; ++k) part += pv[k];
+        acc += part;
     }
     u64 n = nl + gstep * groups;
     for (u64 i = il + 32ull * kS1Unroll * groups; i < i1; i += 32, n += nstep)
