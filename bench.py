@@ -238,16 +238,16 @@ def sieve_marks(u_total, u_dense, sm_count, S=1 << 17):
 
 # Warp instructions per unit of work, from ncu smsp__inst_executed.sum of one launch
 # divided by that launch's work:
-#   sums_kernel at M(10^15) (B200 policy): 7.32e9 instructions for 5.98e9 S1 lookups +
-#     2.40e9 S2 wheel positions; split between the two in the ratio of the timing-only
-#     captures that keep one of the two parts (0.65 and 1.50 predict 7.49e9, 2% above);
+#   sums_kernel at M(10^15) (B200 policy): 7.05e9 instructions for 5.98e9 S1 lookups +
+#     2.40e9 S2 wheel positions; the S2 positions at 1.50 each (timing-only capture that
+#     keeps only the S2 part), the rest, 0.58 per lookup, to S1;
 #   sieve_kernel, odd mode, on the M(10^15) table: 5.63e7 instructions for 1.01e8 values.
-SUMS_INST_PER_S1 = 0.65
+SUMS_INST_PER_S1 = 0.58
 SUMS_INST_PER_S2 = 1.50
 SIEVE_INST_PER_VALUE = 0.556
 # DRAM bytes per op of sums_kernel (dram__bytes_read.sum + dram__bytes_write.sum of one
-# launch over its S1 lookups + S2 positions) at M(10^15): 11.16 GB / 8.38e9 ops.
-SUMS_DRAM_PER_OP = 1.33
+# launch over its S1 lookups + S2 positions) at M(10^15): 10.71 GB / 8.38e9 ops.
+SUMS_DRAM_PER_OP = 1.28
 
 
 def sums_roofline(st, sums_ms, peak, peak_kind, issue_peak, f_mhz):
