@@ -6,8 +6,10 @@
 * random X with randomised parameters against the oracle (any valid
   parameters give the same M(X); the checksums must match at equal ones),
 * boundary inputs: tiny X, X = u, X = u + 1, the dense/compressed quotient
-  boundary X = 99,975,680 (test_sieve.cpp:206-209).
+  boundary X = 99,975,680 (test_sieve.cpp:206-209),
+* M(10^18) under three parameter sets, M(2^63 - 1) under two.
 """
+import math
 import random
 
 import pytest
@@ -145,6 +147,27 @@ def test_m1e18_learned_tuner_params(engine):
         mlp.close()
     assert not fb
     _m1e18(engine, p)
+
+
+def test_int64_max_two_parameter_sets(engine):
+    """M(2^63 - 1), the largest X of the int64 interface, under two parameter sets
+    (u = 2.5e11, cx = 1.25, 120 GB of device data; u = 2e11, cx = 1.5): the splits
+    give different C, S1 and S2 (different tables, split points and term lists) and
+    must give the same M, each with C - S1 - S2 = M (mod 2^64).  No independently
+    computed M is known at this X (the reference's CPU engine would take days); the
+    pinned 580197744 is this engine's value, agreed by both splits."""
+    X = (1 << 63) - 1
+    got = []
+    for cx, u in ((1.25, 250000000000), (1.5, 200000000000)):
+        p = dr_b200.default_params(X, dr_b200.POLICY_GPU)
+        p.cx, p.u_total = cx, u
+        p.mu_limit = int(cx * math.isqrt(X)) + 2000
+        assert dr_b200.check_params(X, p) == 0
+        r = engine.mertens(X, p)
+        assert (r.stats.C - r.stats.S1 - r.stats.S2) % (1 << 64) == r.M % (1 << 64)
+        got.append((r.M, r.stats.C, r.stats.S1, r.stats.S2))
+    assert got[0][0] == got[1][0] == 580197744
+    assert got[0][1:] != got[1][1:]
 
 
 def test_windowed_s1_matches_direct(engine):
