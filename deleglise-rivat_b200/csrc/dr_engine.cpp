@@ -159,6 +159,28 @@ void release(dr_ctx* c, DevBuf& b) {
     b.cap = 0;
 }
 
+// Every device buffer but the constant stencils is scratch of one call (each call
+// rebuilds its table), but buffers only grow, so a context that served a call with
+// other shapes can hold more than the next call leaves room for.  After the work in
+// flight has finished, release them all; returns whether anything was released.
+bool release_scratch(dr_ctx* c) {
+    cudaStreamSynchronize(c->stream);
+    cudaStreamSynchronize(c->side);
+    cudaGetLastError();
+    drop_graphs(c);
+    DevBuf* bufs[] = {&c->dM, &c->planes, &c->ckpt, &c->wheel, &c->seg_sum, &c->seg_off, &c->primes, &c->pinv,
+                      &c->items, &c->queries, &c->ops, &c->prefix, &c->scan_tmp, &c->acc, &c->counts, &c->ticket,
+                      &c->misc, &c->inv, &c->invw, &c->wdesc, &c->witems, &c->slots, &c->prcp, &c->sq_cnt,
+                      &c->sq_off, &c->sq_cur, &c->sq_pos, &c->sq_tmp, &c->items_odd, &c->dplanes};
+    bool any = false;
+    for (DevBuf* b : bufs) {
+        any = any || b->p;
+        release(c, *b);
+    }
+    c->table_valid = false;
+    return any;
+}
+
 // Timing events: under stream capture an event record must be an explicit
 // graph node (cudaEventRecordExternal); a plain record there is only a
 // dependency marker and the event would never complete.
@@ -1015,9 +1037,15 @@ int dr_table_build(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit
     if (!c) return fail(DR_ERR_ARG, "ctx is NULL");
     CU(cudaSetDevice(c->device));
     const double t0 = now_ms();
-    int rc = stage_reserve(c, stage_bytes_for(primes_upto(c, isqrt_i64(std::max<int64_t>(u_total, 0))).size(), 0));
+    const size_t stage = stage_bytes_for(primes_upto(c, isqrt_i64(std::max<int64_t>(u_total, 0))).size(), 0);
+    int rc = stage_reserve(c, stage);
     if (rc) return rc;
     rc = build_table(c, u_total, u_dense, mu_limit, tuning, st);
+    if (rc == DR_ERR_NOMEM && release_scratch(c)) {  // retry once without the buffers of earlier calls
+        if (st) std::memset(st, 0, sizeof(*st));
+        rc = stage_reserve(c, stage);
+        if (!rc) rc = build_table(c, u_total, u_dense, mu_limit, tuning, st);
+    }
     if (rc) return rc;
     CU(cudaStreamSynchronize(c->stream));
     if (st) {
@@ -1087,12 +1115,19 @@ int dr_mertens_batch(dr_ctx* c, const int64_t* X, int64_t count, const dr_params
         }
     }
     const size_t n_primes = primes_upto(c, isqrt_i64(ut)).size();
-    int rc = stage_reserve(c, stage_bytes_for(n_primes, count));
-    if (rc) return rc;
-    rc = build_table(c, ut, ud, ml, &tune, st);
-    if (rc) return rc;
     int launches = 0;
-    rc = enqueue_queries(c, X, P.data(), count, &tune, &launches);
+    int rc = DR_OK;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        // a second attempt only after a budget or allocation failure that released
+        // the buffers kept from earlier, larger calls
+        if (attempt == 1 && !(rc == DR_ERR_NOMEM && release_scratch(c))) break;
+        if (st) std::memset(st, 0, sizeof(*st));
+        launches = 0;
+        rc = stage_reserve(c, stage_bytes_for(n_primes, count));
+        if (!rc) rc = build_table(c, ut, ud, ml, &tune, st);
+        if (!rc) rc = enqueue_queries(c, X, P.data(), count, &tune, &launches);
+        if (!rc) break;
+    }
     if (rc) return rc;
     rc = finish_queries(c, X, count, launches, c->stage_used + c->wstage_used, out, st);
     if (rc) return rc;

@@ -92,7 +92,10 @@ typedef struct {
 int dr_ctx_create(int device, void *cuda_stream /* NULL: own stream */, dr_ctx **out);
 int dr_ctx_destroy(dr_ctx *ctx);
 const char *dr_last_error(void);
-/* Cap on device bytes the context may hold (0: 90% of free memory at create). */
+/* Cap on device bytes the context may hold (0: 92% of the free memory plus what the
+ * context holds).  Buffers grow to the largest call served and are kept; a call that
+ * would exceed the cap first releases them (after the work in flight) and runs once
+ * more, so only a call that does not fit on its own fails with DR_ERR_NOMEM. */
 int dr_ctx_set_hbm_budget(dr_ctx *ctx, uint64_t bytes);
 int dr_device_info(int device, int *sm_count, uint64_t *hbm_bytes);
 
