@@ -459,9 +459,14 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
         if (forks < dr_ctx::kForks - 1 || li + 1 == plan.size()) {
             CU(cudaEventRecord(c->fork[forks], c->stream));
             CU(cudaStreamWaitEvent(c->side, c->fork[forks], 0));
-            launch_seg_scan_range((const int32_t*)c->seg_sum.p, (int32_t*)c->seg_off.p, fixed, l.end, c->side);
+            // beside a sieve launch the scan and fix-up stay small (one sieve CTA fills an
+            // SM's shared memory, not its threads); after the last one they are the tail
+            // of the build and take the whole GPU
+            const bool last = li + 1 == plan.size();
+            launch_seg_scan_range((const int32_t*)c->seg_sum.p, (int32_t*)c->seg_off.p, fixed, l.end,
+                                  last ? 1024 : 256, c->side);
             launch_fixup_range((int16_t*)c->dM.p, u_dense, S, (const int32_t*)c->seg_off.p, (int32_t*)c->ckpt.p,
-                               nwords, dense_segs, fixed, l.end, c->sm_count * 2, c->side);
+                               nwords, dense_segs, fixed, l.end, c->sm_count * (last ? 16 : 2), c->side);
             CU(cudaGetLastError());
             fixed = l.end;
             ++forks;

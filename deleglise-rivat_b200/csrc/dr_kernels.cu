@@ -895,8 +895,8 @@ void launch_seg_scan(const int32_t* in, int32_t* out, i64 n, cudaStream_t s) {
     seg_scan_kernel<<<1, 1024, 0, s>>>(in, out, 0, n);
 }
 
-void launch_seg_scan_range(const int32_t* in, int32_t* out, i64 b0, i64 b1, cudaStream_t s) {
-    if (b1 > b0) seg_scan_kernel<<<1, 256, 0, s>>>(in, out, b0, b1);
+void launch_seg_scan_range(const int32_t* in, int32_t* out, i64 b0, i64 b1, int threads, cudaStream_t s) {
+    if (b1 > b0) seg_scan_kernel<<<1, threads, 0, s>>>(in, out, b0, b1);
 }
 
 // Adds the segment offsets to the dense prefix values of the 8-value groups [g0, g1)

@@ -127,8 +127,8 @@ size_t sieve_smem_bytes(int S, bool odd);
 // Segment offsets out[i] = sum of in[j < i] for i <= n (out holds n + 1 entries).
 void launch_seg_scan(const int32_t* in, int32_t* out, i64 n, cudaStream_t s);
 // The same for the segments [b0, b1) given out[b0] (written by the range before,
-// 0 for b0 = 0); also writes out[b1].
-void launch_seg_scan_range(const int32_t* in, int32_t* out, i64 b0, i64 b1, cudaStream_t s);
+// 0 for b0 = 0); also writes out[b1].  One CTA of `threads` (32 .. 1024, a multiple of 32).
+void launch_seg_scan_range(const int32_t* in, int32_t* out, i64 b0, i64 b1, int threads, cudaStream_t s);
 // Offsets added to the dense prefix and the checkpoints of the segments [b0, b1).
 void launch_fixup_range(int16_t* dM, i64 u_dense, int S, const int32_t* seg_off, int32_t* ckpt, i64 nwords,
                         i64 dense_segs, i64 b0, i64 b1, int blocks, cudaStream_t s);
