@@ -1188,7 +1188,7 @@ __device__ __forceinline__ double u32_to_double(uint32_t v) {
 // k*nstep*r0), relative error (k*nstep/nfirst)^2 <= (7/256)^2 = 2^-10.4, and two Newton steps
 // r += r*(1 - n*r) square that error twice (to below 2^-41, on the FP64 pipe,
 // which the loop leaves idle) -- far inside what the 32-bit dense route needs
-// (q <= u_dense < 2^31).  Below that every reciprocal is loaded.  This cuts the
+// (q < 2^32).  Below that every reciprocal is loaded.  This cuts the
 // L2 traffic of the reciprocal table by a factor kS1Unroll where the loop is
 // bound by it.
 __device__ __forceinline__ void rcp_group(const double* rcp, uint32_t nfirst, uint32_t nstep, double nstep_d,
@@ -1236,7 +1236,7 @@ __device__ __forceinline__ void rcp_group(const double* rcp, uint32_t nfirst, ui
 // so a warp's reciprocal and table latencies overlap its own arithmetic instead of
 // adding up group after group.  A group
 // whose divisors are tabulated and below 2^31 and whose first (largest) quotient
-// is in the dense tier -- q falls as n grows, so then every quotient is -- runs on
+// is in the dense tier and below 2^32 - 1 -- q falls as n grows, so then every quotient is -- runs on
 // 32-bit quotients (qest/qfix); the rest use the 64-bit routine (every q here is
 // at most u_total < 2^42, inside udiv_rcp's domain) or udiv above the tables.
 __device__ __forceinline__ i64 s1_part(const SumsArgs& a, u64 y, i64 n0, int stride, u64 i0, u64 i1, int lane) {
@@ -1249,7 +1249,9 @@ __device__ __forceinline__ i64 s1_part(const SumsArgs& a, u64 y, i64 n0, int str
     const double nstep_d = u32_to_double(nstep);
     const double yd = __ull2double_rn(y);
     const uint32_t ylo = (uint32_t)y;
-    const double dense_t = 4503599627370496.0 + (double)a.T.u_dense;  // 2^52 + u_dense
+    // 2^52 + the largest quotient of the 32-bit dense route: q <= u_dense and q < 2^32 - 1
+    // (the dense tier may reach 7.6e9 values; larger quotients take the 64-bit route)
+    const double dense_t = 4503599627370496.0 + (double)min(a.T.u_dense, (i64)0xFFFFFFFEll);
     const int16_t* dMm1 = a.T.dM - 1;                                  // dMm1[q] = M(q)
     const u64 il = i0 + (u64)lane;
     // this lane's full groups: il + 32*kS1Unroll*g + 32*(kS1Unroll-1) < i1
@@ -1286,7 +1288,7 @@ __device__ __forceinline__ i64 s1_part(const SumsArgs& a, u64 y, i64 n0, int str
                     pv[k] = __ldg(dMm1 + qq[k]);
                 }
                 acc += part;
-            } else {  // compressed tier (rare): exact tabulated reciprocals for udiv_rcp
+            } else {  // compressed tier or q >= 2^32 - 1 (rare): exact tabulated reciprocals, udiv_rcp
 #pragma unroll
                 for (int k = 0; k < kS1Unroll; ++k) {
                     const uint32_t n = nf + nstep * (uint32_t)k;

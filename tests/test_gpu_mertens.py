@@ -170,6 +170,20 @@ def test_int64_max_two_parameter_sets(engine):
     assert got[0][1:] != got[1][1:]
 
 
+def test_dense_tier_above_2_32(engine):
+    """A dense int16 tier beyond 2^32 values (up to the int16 prefix's 7.6e9): S1 lookups
+    with quotients in (2^32, u_dense] read the dense tier through the 64-bit route.  How
+    the table is split into tiers changes no sum, so C, S1 and S2 equal those of the
+    B200 policy's 4e9-value dense tier."""
+    X = 10**17
+    p = dr_b200.default_params(X, dr_b200.POLICY_GPU)
+    assert p.u_dense <= (1 << 32) < 5000000000 < p.u_total
+    q = dr_b200.Params(**{**p.as_dict(), "u_dense": 5000000000})
+    r0, r1 = engine.mertens(X, p), engine.mertens(X, q)
+    assert r0.M == r1.M == -21830254
+    assert (r0.stats.C, r0.stats.S1, r0.stats.S2) == (r1.stats.C, r1.stats.S1, r1.stats.S2)
+
+
 def test_windowed_s1_matches_direct(engine):
     """The windowed S1 (s1win_kernel) and the sums kernel's direct S1 split every S1
     lookup between them; with the window switched off the sums kernel takes them
