@@ -59,6 +59,30 @@ def test_random_params_vs_oracle(engine, oracle):
         assert (r.M, r.stats.C, r.stats.S1, r.stats.S2) == (o["M"], o["C"], o["S1"], o["S2"]), (X, q)
 
 
+def test_random_params_large_x(engine):
+    """Any valid parameters give the same M(X): M(10^15) under seeded random splits over
+    the whole valid range -- cx 0.4 .. 3, u from its lower limit up to 2e10, the dense tier
+    anywhere from 0 to all of u (beyond 2^32 values where u allows), mu_limit anywhere
+    between its lower limit and u, segments 2^15 .. 2^18 -- each with C - S1 - S2 = M."""
+    X, want = 10**15, -3216373
+    rng = random.Random(20261204)
+    done = 0
+    while done < 16:
+        cx = rng.uniform(0.4, 3.0)
+        A = int(cx * math.isqrt(X))
+        lo = max(A + 2, 3 * math.isqrt(X))
+        u = int(math.exp(rng.uniform(math.log(lo), math.log(2e10))))
+        ud = rng.choice([0, u, rng.randint(0, u), min(u, 5000000000)])
+        ml = rng.randint(min(u, max(A, X // u) + 1), u)
+        p = dr_b200.Params(u_total=u, u_dense=ud, cx=cx, mu_limit=ml, segment_log2=rng.choice([15, 16, 17, 18]))
+        if dr_b200.check_params(X, p) != 0 or dr_b200.query_bytes(X, p) > (48 << 30):
+            continue
+        r = engine.mertens(X, p)
+        assert r.M == want, p
+        assert (r.stats.C - r.stats.S1 - r.stats.S2) % (1 << 64) == want % (1 << 64), p
+        done += 1
+
+
 def test_small_and_boundary_inputs(engine, oracle):
     for X in list(range(0, 200)) + [1000, 10**5, 10**5 + 1, 5 * 10**7, 5 * 10**7 + 1, 99975680]:
         want = oracle.mertens(X) if X > 0 else 0
