@@ -353,11 +353,11 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     a.sq_first = first_at_least(5);
     a.w_first = first_at_least(13);
     // B sieved bytes per segment (S in full mode, S/2 in odd mode): warp items for the
-    // moduli below B/32, one thread per prime above
+    // moduli below B/kItemDiv, one thread per prime above
     auto set_moduli = [&](SieveArgs& m, int B, DevBuf& buf) -> int {
-        m.tierB_first = std::max(m.w_first, first_at_least((uint32_t)std::max(13, B / 32)));
-        int k = m.sq_first;  // first prime whose square reaches B/32
-        while (k < (int)pr.size() && (uint64_t)pr[k] * pr[k] < (uint64_t)(B / 32)) ++k;
+        m.tierB_first = std::max(m.w_first, first_at_least((uint32_t)std::max(13, B / kItemDiv)));
+        int k = m.sq_first;  // first prime whose square reaches B/kItemDiv
+        while (k < (int)pr.size() && (uint64_t)pr[k] * pr[k] < (uint64_t)(B / kItemDiv)) ++k;
         m.sqB_first = k;
         std::vector<uint4> items(kMaxSieveItems);
         m.n_items = build_sieve_items(pr.data(), (int)pr.size(), B, items.data(), kMaxSieveItems);

@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
             const uint32_t pidx = I.w & 0x7fffffffu;
             mark_item<ODD>(buf32, I, (I.w >> 31) ? __ldg(a.sqinv + pidx) : __ldg(a.pinv + pidx), low, nb, lane);
         }
-        //    Larger moduli (at most 32 hits per segment): one prime per thread.
+        //    Larger moduli (at most kItemDiv hits per segment): one prime per thread.
         //    Squares above S hit a segment at most once: their hits come from
         //    the per-segment bucket (sq_off / sq_pos: value offsets) when there is one.
         const int sq_end = a.sq_off ? a.sqC_first : a.n_primes;
@@ -686,7 +686,7 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
 }
 
 int build_sieve_items(const uint32_t* primes, int n_primes, int S, uint4* out, int cap) {
-    const uint32_t lim = (uint32_t)(S / 32);
+    const uint32_t lim = (uint32_t)(S / kItemDiv);
     int n = 0;
     for (int i = 0; i < n_primes; ++i) {
         const uint32_t p = primes[i];

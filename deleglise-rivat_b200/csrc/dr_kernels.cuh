@@ -35,8 +35,8 @@ struct SieveArgs {
     int n_primes;       // primes <= isqrt(u_total), ascending
     int sq_first;       // first prime >= 5 (square flags)
     int w_first;        // first prime >= 13 (weights)
-    int tierB_first;    // first prime whose weights are marked thread-per-prime (p >= S/32)
-    int sqB_first;      // first prime whose square is marked thread-per-prime (p^2 >= S/32)
+    int tierB_first;    // first prime whose weights are marked thread-per-prime (p >= B/kItemDiv)
+    int sqB_first;      // first prime whose square is marked thread-per-prime (p^2 >= B/kItemDiv)
     int n_items;        // warp work items for the smaller moduli (see build_sieve_items)
     const uint4* items; // {modulus, start offset, weight or 0x80, prime index | square bit 31}
     const uint32_t* primes;
@@ -110,8 +110,14 @@ void launch_sq_bucket_count(const uint32_t* primes, int first, int n, i64 u_tota
 void launch_sq_bucket_fill(const uint32_t* primes, int first, int n, i64 u_total, i64 u_dense, i64 dense_segs,
                            int lgS, const u64* off, u64* cur, uint32_t* pos, cudaStream_t s);
 
+// Moduli with at least kItemDiv hits in the B bytes a segment sieves (m < B/kItemDiv)
+// are marked by warp work items, larger ones one prime per thread (at most kItemDiv
+// hits each).  64 measured best: the M(10^16) table takes 20.36 ms against 20.68 ms
+// with 32 and 21.10 ms with 24 (48: 20.36 ms).
+constexpr int kItemDiv = 64;
+
 // Warp work items for the sieve's smaller moduli: the multiples of every prime
-// 13 <= p < S/32 (log weights) and of every square p^2 < S/32, p >= 5 (flags),
+// 13 <= p < S/kItemDiv (log weights) and of every square p^2 < S/kItemDiv, p >= 5 (flags),
 // cut into pieces of at most 1024 hits (32 lanes x 32 strides), so that the
 // warps of a CTA get equal shares of the marking instead of one warp holding
 // p = 13.  Items are ordered by prime index: the items valid for the first n

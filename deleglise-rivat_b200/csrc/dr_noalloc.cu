@@ -262,8 +262,8 @@ extern "C" int dr_table_build_noalloc(int device, void* stream, int64_t u_total,
         a.n_primes = count_primes_upto(root);
         a.sq_first = std::min(a.n_primes, count_primes_upto(4));
         a.w_first = std::min(a.n_primes, count_primes_upto(12));
-        a.tierB_first = std::max(a.w_first, std::min(a.n_primes, count_primes_upto(S / 32 - 1)));
-        a.sqB_first = std::max(a.sq_first, std::min(a.n_primes, count_primes_upto(isqrt_exact(S / 32 - 1))));
+        a.tierB_first = std::max(a.w_first, std::min(a.n_primes, count_primes_upto(S / kItemDiv - 1)));
+        a.sqB_first = std::max(a.sq_first, std::min(a.n_primes, count_primes_upto(isqrt_exact(S / kItemDiv - 1))));
         a.n_items = sieve_items_prefix(g_host_items, g_host_item_count, a.n_primes);
         a.items = (const uint4*)(d.scratch + kOffItems);
         a.primes = d.scratch + kOffPrimes;
