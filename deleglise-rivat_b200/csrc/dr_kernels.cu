@@ -255,13 +255,13 @@ __device__ __forceinline__ void planes_odd_mode(const SieveArgs& a, const uint32
 }
 
 // Marks of one warp item I from its first hit at byte j0 (lane l takes j0 + l*m, then
-// every 32nd multiple, up to the item's 1024 hits or the end of the sieved bytes).
+// every 32nd multiple, up to the item's kItemHits hits or the end of the sieved bytes).
 // A lane's strides are 32*m bytes, a multiple of 4: its byte position within the
 // 32-bit word, and so the shifted mark, stays the same, and the word advances by 8*m.
 __device__ __forceinline__ void mark_item_from(uint32_t* buf32, const uint4 I, uint32_t j0, int nb, int lane) {
     const uint32_t m = I.x;
     const uint32_t j = j0 + (uint32_t)lane * m;
-    const uint32_t jend = min((uint32_t)nb, I.y + 1024u * m);
+    const uint32_t jend = min((uint32_t)nb, I.y + (uint32_t)kItemHits * m);
     const uint32_t ph = j & 3u;
     // byte 4*(p - buf32) + ph < jend  <=>  p - buf32 < (jend - ph + 3) / 4
     const uint32_t wend = jend + 3u >= ph ? (jend + 3u - ph) >> 2 : 0u;
@@ -300,7 +300,7 @@ __device__ __forceinline__ void mark_prime(uint32_t* buf32, uint32_t j, uint32_t
 
 // Marks of one warp item I = {modulus m, first byte, weight or 0x80, prime index |
 // square bit 31}: lanes stride the multiples of m at or after byte I.y (ODD: the odd
-// multiples, m bytes apart), 32 strides each, with the 64-bit reciprocal inv of m.
+// multiples, m bytes apart), kItemHits/32 strides each, with the 64-bit reciprocal inv of m.
 template <bool ODD>
 __device__ __forceinline__ void mark_item(uint32_t* buf32, const uint4 I, const u64 inv, i64 low, int nb,
                                           int lane) {
@@ -692,14 +692,14 @@ int build_sieve_items(const uint32_t* primes, int n_primes, int S, uint4* out, i
         const uint32_t p = primes[i];
         if (p >= 13 && p < lim) {
             const uint32_t w = (32u - (uint32_t)__builtin_clz(p - 1)) | 1u;
-            for (uint32_t st = 0; st < (uint32_t)S; st += 1024u * p) {
+            for (uint32_t st = 0; st < (uint32_t)S; st += (uint32_t)kItemHits * p) {
                 if (n >= cap) return -1;  // an item would be dropped: its marks would be missing
                 out[n++] = make_uint4(p, st, w, (uint32_t)i);
             }
         }
         if (p >= 5 && p * p < lim) {
             const uint32_t q = p * p;
-            for (uint32_t st = 0; st < (uint32_t)S; st += 1024u * q) {
+            for (uint32_t st = 0; st < (uint32_t)S; st += (uint32_t)kItemHits * q) {
                 if (n >= cap) return -1;
                 out[n++] = make_uint4(q, st, 0x80u, (uint32_t)i | 0x80000000u);
             }

@@ -115,10 +115,13 @@ void launch_sq_bucket_fill(const uint32_t* primes, int first, int n, i64 u_total
 // hits each).  64 measured best: the M(10^16) table takes 20.36 ms against 20.68 ms
 // with 32 and 21.10 ms with 24 (48: 20.36 ms).
 constexpr int kItemDiv = 64;
+// Hits per warp item: 2048 measured best (the M(10^16) table: 20.04 ms against 20.41 with
+// 1024, 20.56 with 512, 20.30 with 4096, 20.46 with 8192).
+constexpr int kItemHits = 2048;
 
 // Warp work items for the sieve's smaller moduli: the multiples of every prime
 // 13 <= p < S/kItemDiv (log weights) and of every square p^2 < S/kItemDiv, p >= 5 (flags),
-// cut into pieces of at most 1024 hits (32 lanes x 32 strides), so that the
+// cut into pieces of at most kItemHits hits (32 lanes x 64 strides), so that the
 // warps of a CTA get equal shares of the marking instead of one warp holding
 // p = 13.  Items are ordered by prime index: the items valid for the first n
 // primes are a prefix.  Returns the count written (<= cap), or -1 if the items
