@@ -211,6 +211,18 @@ def run_reference(args, world, rank):
 KNOWN = {10**k: m for k, m in [(9, -222), (10, -33722), (11, -87856), (12, 62366), (13, 599582), (14, -875575),
                                     (15, -3216373), (16, -3195437), (17, -21830254), (18, -46758740)]}
 # test_dr.cpp, test_cuda.cu, README; 10^18 pinned by the reference engine built from its own sources
+KNOWN[(1 << 63) - 1] = 580197744  # this engine's value, agreed by two parameter sets (no reference value)
+
+
+def with_table_size(p, X, u):
+    """The B200 policy's parameters with the table size set to u: the dense tier by the
+    policy's rule (max(1.28e8, u/16), at most 4e9) and mu_limit covering A and X/u."""
+    import dr_b200
+
+    dense = min(4000000000, max(128000000, u // 16))
+    dense = min(u, (dense + 255) & ~255)
+    a_max = int(p.cx * X**0.5) + 1000
+    return dr_b200.Params(**{**p.as_dict(), "u_total": u, "u_dense": dense, "mu_limit": min(u, max(a_max, X // u + 1000))})
 
 
 def sieve_marks(u_total, u_dense, sm_count, S=1 << 17):
@@ -339,6 +351,13 @@ def run_engine(args, world, rank, local):
     want = KNOWN.get(X)
     tuned = dr_b200.default_params(X, dr_b200.POLICY_REFERENCE if args.policy == "reference" else dr_b200.POLICY_GPU)
     default = dr_b200.default_params(X, dr_b200.POLICY_REFERENCE)
+    if args.u:
+        tuned = with_table_size(tuned, X, int(float(args.u)))
+    stream = None
+    if args.resident:
+        # streamed table: M held up to the resident limit, the rest sieved band by band
+        stream = {"u_resident": int(float(args.resident)), "band_values": int(float(args.band or 0))}
+        eng.set_resident_limit(stream["u_resident"], stream["band_values"])
 
     def check(m):
         if want is not None and m != want:
@@ -378,14 +397,18 @@ def run_engine(args, world, rank, local):
     sec_per, host_per, stats = timed(tuned, args.steps, clocks)
     value = sec_per / world  # whole job: N replicas finish N results in sec_per
 
+    if stream:
+        eng.set_resident_limit(0)  # the comparison arms hold their tables whole
     # the plain path with the reference's default parameters, same run
-    check(eng.mertens(X, default).M)
-    dsec, dhost, dstats = timed(default, max(1, args.steps // 2))
+    dsec = dhost = None
+    if not args.no_compare:
+        check(eng.mertens(X, default).M)
+        dsec, dhost, dstats = timed(default, max(1, args.steps // 2))
 
     # the learned tuner's proposal (committed weights), same run
     learned = None
     wpath = os.path.join(ROOT, "deleglise-rivat_b200", "dr_b200", "tuner_weights.json")
-    if os.path.exists(wpath):
+    if os.path.exists(wpath) and not args.no_compare:
         import numpy as np
 
         mlp = dr_b200.MLP(eng)
@@ -465,7 +488,8 @@ def run_engine(args, world, rank, local):
     f_mhz = clk["sm_mhz"] or clk["sm_max_mhz"] or 1965.0
     issue_peak = sms * 4 * f_mhz * 1e6
     roofline = sums_roofline(s0_, sums, peak, peak_kind, issue_peak, f_mhz)
-    table_roofline = sieve_roofline(tuned, tab, peak, peaks_int, issue_peak, sms)
+    # a streamed table's bands are built inside the sums phase: no table-phase roofline
+    table_roofline = None if stream else sieve_roofline(tuned, tab, peak, peaks_int, issue_peak, sms)
     line = {
         "metric": "sec per M(10^16)" if X == X_HEADLINE else f"sec per M({X})", "value": value, "unit": "s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_per * 1e3,
@@ -476,8 +500,9 @@ def run_engine(args, world, rank, local):
                    "l2": "inputs larger than L2 (table and reciprocals rebuilt each step)",
                    "parallelism": f"replicas x{world}"},
         "phases_ms": phases,
-        "default_params": {"ms_per_step": dsec * 1e3, "u_total": default.u_total, "cx": default.cx,
-                           "tuned_speedup": dsec / sec_per, "e2e_s": dhost},
+        "default_params": None if dsec is None else {"ms_per_step": dsec * 1e3, "u_total": default.u_total,
+                                                     "cx": default.cx, "tuned_speedup": dsec / sec_per, "e2e_s": dhost},
+        "stream": stream,
         "learned_tuner": learned,
         "gpu_launches": launches,
         "e2e": {"value": host_per / world, "unit": "s", "h2d_bytes_per_step": int(s0_.h2d_bytes),
@@ -507,6 +532,10 @@ def main():
     ap.add_argument("--table", default=None, help="time the table build only: u_total[,u_dense[,mu_limit]]")
     ap.add_argument("--seg", type=int, default=0, help="sieve segment = 2^seg values (0: default)")
     ap.add_argument("--block", type=int, default=0, help="sieve threads per CTA (0: default)")
+    ap.add_argument("--u", default=None, help="table size u_total (dense tier and mu_limit by the B200 policy's rule)")
+    ap.add_argument("--resident", default=None, help="stream the table above this many values (dr_ctx_set_resident_limit)")
+    ap.add_argument("--band", default=None, help="values per streamed band (0: the resident compressed tier's size)")
+    ap.add_argument("--no-compare", action="store_true", help="skip the default-parameter and learned-tuner arms")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

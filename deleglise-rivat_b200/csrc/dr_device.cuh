@@ -168,13 +168,14 @@ struct TableView {
     const int32_t* ckpt;
     const uint4* wheel;
     i64 u_dense, u_total, mu_limit;
+    i64 cbase;  // compressed-tier word held in planes[0] / ckpt[0]: 0, or a streamed band's first word
 };
 
 #ifdef __CUDACC__
 __device__ __forceinline__ int32_t table_M(const TableView& t, u64 q) {
     if (q <= (u64)t.u_dense) return q ? (int32_t)__ldg(t.dM + (q - 1)) : 0;
     const u64 off = q - (u64)t.u_dense - 1;
-    const u64 w = off >> 6;
+    const u64 w = (off >> 6) - (u64)t.cbase;
     const ulonglong2 p = __ldg(t.planes + w);
     const int32_t c = __ldg(t.ckpt + w);
     const u64 mask = ~0ull >> (63 - (off & 63));
@@ -269,6 +270,16 @@ __device__ __forceinline__ i64 wheel_upper(i64 n) {
 
 #endif  // __CUDACC__
 
+// The S1 lookups one planning pass keeps: those with qlo <= floor(y/n) <= qhi.  A table
+// streamed in bands (the compressed tier above u_resident never held whole) is summed
+// in passes: the resident pass keeps q <= u_resident with S2 and the constant parts,
+// each band pass the q of its band and nothing else (s1_only).  Every lookup falls in
+// exactly one pass, so the S1 total is the same sum of the same terms.
+struct S1Band {
+    u64 qlo, qhi;  // whole table: 0, ~0
+    int s1_only;
+};
+
 // Index ranges of one evaluation in op order: S1 segments first, then S2 pieces.
 struct EvalDesc {
     u64 y;
@@ -291,7 +302,8 @@ struct EvalDesc {
 
 // One evaluation slot as the planner leaves it for the sums kernel (96 bytes): y, the
 // split points, the S1 segments and, in `bits`, the kind (bits 0-1), the sign of the
-// coefficient (bit 2) and per S1 segment g a stride code and sign (bits 3+3g ..).
+// coefficient (bit 2), per S1 segment g a stride code and sign (bits 3+3g ..) and
+// kSlotS1Only (a band pass of a streamed table: S1 lookups only, no S2 pieces).
 struct __align__(16) SlotDesc {
     u64 y;
     i64 A, B;
@@ -300,6 +312,7 @@ struct __align__(16) SlotDesc {
     u64 bits;
 };
 static_assert(sizeof(SlotDesc) == 96, "SlotDesc is six 16-byte words");
+constexpr u64 kSlotS1Only = 1ull << 15;
 
 #ifdef __CUDACC__
 __device__ __forceinline__ i64 piece_mcount(i64 lo, i64 hi) {
@@ -375,7 +388,35 @@ __device__ __forceinline__ void eval_total(EvalDesc& d) {
 // 3*clo >= s0, 3*chi <= kappa_y -- both are dropped: the first evaluation keeps its
 // odd n coprime to 3 (the wheel) and the multiples of 3 outside [3clo, 3chi], the
 // second its divisors outside [clo, chi].  The S1 total is unchanged term for term.
-__device__ inline void decode_eval(const QueryDev& Q, const TableView& T, i64 c, int e, EvalDesc& d) {
+__device__ __forceinline__ void s1_band_cut(EvalDesc& d, const S1Band& band) {
+    const u64 y = d.y;
+    // n >= nlo <=> q <= qhi;  n <= nhi <=> q >= qlo (and n <= y: q >= 1)
+    const i64 nlo = band.qhi >= y ? 1 : (i64)udiv(y, band.qhi + 1) + 1;
+    const i64 nhi = band.qlo <= 1 ? (i64)y : (i64)udiv(y, band.qlo);
+    for (int g = 0; g < kS1Seg; ++g) {
+        const i64 cnt = d.s1_cnt[g], n0 = d.s1_n0[g];
+        if (cnt <= 0) continue;
+        const int st = d.s1_stride[g];
+        if (st == S1_WHEEL) {  // n0: wheel index
+            const i64 first = max(n0, wheel_lower(nlo));
+            const i64 last = min(n0 + cnt - 1, wheel_upper(nhi));
+            d.s1_n0[g] = first;
+            d.s1_cnt[g] = last >= first ? last - first + 1 : 0;
+        } else {
+            const i64 ia = nlo > n0 ? (nlo - n0 + st - 1) / st : 0;
+            const i64 ib = nhi >= n0 ? min(cnt - 1, (nhi - n0) / st) : -1;
+            d.s1_n0[g] = n0 + st * ia;
+            d.s1_cnt[g] = ib >= ia ? ib - ia + 1 : 0;
+        }
+    }
+    if (band.s1_only) {
+        d.npieces = 0;
+        d.nseg = kS1Seg;
+    }
+}
+
+__device__ inline void decode_eval(const QueryDev& Q, const TableView& T, i64 c, int e, EvalDesc& d,
+                                   const S1Band band = S1Band{0, ~0ull, 0}) {
     d.kind = EVAL_NONE;
     d.total = 0;
     d.nseg = 0;
@@ -460,6 +501,7 @@ __device__ inline void decode_eval(const QueryDev& Q, const TableView& T, i64 c,
         s1_set(d, 3, e0, 2, last, sg);
         eval_pieces(d);
     }
+    if (band.qlo > 1 || band.qhi < (u64)Q.u || band.s1_only) s1_band_cut(d, band);
     // windowed S1: the lookups with q < wc*W, i.e. n > y/(wc*W), go to s1win_kernel
     for (int g = 0; g < kS1Seg; ++g) {
         d.s1_full[g] = d.s1_cnt[g];
@@ -498,7 +540,7 @@ __device__ __forceinline__ void pack_slot(const EvalDesc& d, SlotDesc* out) {
     s.y = d.y;
     s.A = d.A;
     s.B = d.kind == EVAL_COMB2 ? d.B : 0;
-    u64 bits = (u64)d.kind | (d.coef < 0 ? 4ull : 0ull);
+    u64 bits = (u64)d.kind | (d.coef < 0 ? 4ull : 0ull) | (d.npieces == 0 ? kSlotS1Only : 0ull);
     for (int g = 0; g < kS1Seg; ++g) {
         s.n0[g] = d.s1_n0[g];
         s.cnt[g] = d.s1_cnt[g];
@@ -529,6 +571,10 @@ __device__ __forceinline__ void unpack_slot(const SlotDesc& s, EvalDesc& d) {
         return;
     }
     eval_pieces(d);
+    if (s.bits & kSlotS1Only) {
+        d.npieces = 0;
+        d.nseg = kS1Seg;
+    }
     eval_total(d);
 }
 

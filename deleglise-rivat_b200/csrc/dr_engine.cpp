@@ -71,6 +71,10 @@ struct dr_ctx {
     DevBuf dM, planes, ckpt, wheel, seg_sum, seg_off, primes, pinv, items, stencil, prcp;
     DevBuf items_odd, stencil_odd, dplanes;  // odd-mode sieve: items, stencil, dense-tier plane words
     DevBuf sq_cnt, sq_off, sq_cur, sq_pos, sq_tmp;  // bucketed square hits per segment
+    // streamed table (dr_ctx_set_resident_limit): above u_resident the compressed tier
+    // is built and consumed band by band in these two buffers, never held whole
+    DevBuf bplanes, bckpt;
+    int64_t u_resident = 0, band_values = 0;
     // query buffers
     DevBuf queries, ops, prefix, scan_tmp, acc, counts, ticket, misc, inv, invw, wdesc, witems, slots;
     // table state
@@ -171,7 +175,8 @@ bool release_scratch(dr_ctx* c) {
     DevBuf* bufs[] = {&c->dM, &c->planes, &c->ckpt, &c->wheel, &c->seg_sum, &c->seg_off, &c->primes, &c->pinv,
                       &c->items, &c->queries, &c->ops, &c->prefix, &c->scan_tmp, &c->acc, &c->counts, &c->ticket,
                       &c->misc, &c->inv, &c->invw, &c->wdesc, &c->witems, &c->slots, &c->prcp, &c->sq_cnt,
-                      &c->sq_off, &c->sq_cur, &c->sq_pos, &c->sq_tmp, &c->items_odd, &c->dplanes};
+                      &c->sq_off, &c->sq_cur, &c->sq_pos, &c->sq_tmp, &c->items_odd, &c->dplanes, &c->bplanes,
+                      &c->bckpt};
     bool any = false;
     for (DevBuf* b : bufs) {
         any = any || b->p;
@@ -281,6 +286,7 @@ TableView view_of(dr_ctx* c) {
     T.u_dense = c->t_u_dense;
     T.u_total = c->t_u_total;
     T.mu_limit = c->t_mu_limit;
+    T.cbase = 0;
     return T;
 }
 
@@ -293,6 +299,30 @@ int check_table_limits(int64_t u_total, int64_t u_dense, int64_t mu_limit) {
     if (mu_limit < 0 || mu_limit > u_total)
         return fail(DR_ERR_PARAMS, "mu_limit must be in [0, u_total] (got %lld)", (long long)mu_limit);
     if (u_total > (int64_t)4000000000000LL) return fail(DR_ERR_PARAMS, "u_total above 4e12 is not supported");
+    return DR_OK;
+}
+
+// The sieve's moduli for B sieved bytes per segment (S in full mode, S/2 in odd mode):
+// warp items for the moduli below B/kItemDiv (uploaded into buf), one thread per prime
+// above.  m.w_first and m.sq_first must be set.
+int set_sieve_moduli(dr_ctx* c, const std::vector<uint32_t>& pr, int B, SieveArgs& m, DevBuf& buf) {
+    m.tierB_first = std::max(m.w_first, (int)(std::lower_bound(pr.begin(), pr.end(),
+                                                                (uint32_t)std::max(13, B / kItemDiv)) - pr.begin()));
+    int k = m.sq_first;  // first prime whose square reaches B/kItemDiv
+    while (k < (int)pr.size() && (uint64_t)pr[k] * pr[k] < (uint64_t)(B / kItemDiv)) ++k;
+    m.sqB_first = k;
+    std::vector<uint4> items(kMaxSieveItems);
+    m.n_items = build_sieve_items(pr.data(), (int)pr.size(), B, items.data(), kMaxSieveItems);
+    if (m.n_items < 0) return fail(DR_ERR_PARAMS, "sieve work items exceed %d for %d bytes per segment", kMaxSieveItems, B);
+    int e = ensure(c, buf, (size_t)std::max(m.n_items, 1) * 16);
+    if (e) return e;
+    if (m.n_items) {
+        const void* si = stage_put(c, items.data(), (size_t)m.n_items * 16);
+        if (!si) return fail(DR_ERR_NOMEM, "internal: staging area too small");
+        if (cudaMemcpyAsync(buf.p, si, (size_t)m.n_items * 16, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+            return fail(DR_ERR_CUDA, "sieve items upload failed");
+    }
+    m.items = (const uint4*)buf.p;
     return DR_OK;
 }
 
@@ -352,27 +382,7 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     };
     a.sq_first = first_at_least(5);
     a.w_first = first_at_least(13);
-    // B sieved bytes per segment (S in full mode, S/2 in odd mode): warp items for the
-    // moduli below B/kItemDiv, one thread per prime above
-    auto set_moduli = [&](SieveArgs& m, int B, DevBuf& buf) -> int {
-        m.tierB_first = std::max(m.w_first, first_at_least((uint32_t)std::max(13, B / kItemDiv)));
-        int k = m.sq_first;  // first prime whose square reaches B/kItemDiv
-        while (k < (int)pr.size() && (uint64_t)pr[k] * pr[k] < (uint64_t)(B / kItemDiv)) ++k;
-        m.sqB_first = k;
-        std::vector<uint4> items(kMaxSieveItems);
-        m.n_items = build_sieve_items(pr.data(), (int)pr.size(), B, items.data(), kMaxSieveItems);
-        if (m.n_items < 0) return fail(DR_ERR_PARAMS, "sieve work items exceed %d for %d bytes per segment", kMaxSieveItems, B);
-        int e = ensure(c, buf, (size_t)std::max(m.n_items, 1) * 16);
-        if (e) return e;
-        if (m.n_items) {
-            const void* si = stage_put(c, items.data(), (size_t)m.n_items * 16);
-            if (!si) return fail(DR_ERR_NOMEM, "internal: staging area too small");
-            if (cudaMemcpyAsync(buf.p, si, (size_t)m.n_items * 16, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
-                return fail(DR_ERR_CUDA, "sieve items upload failed");
-        }
-        m.items = (const uint4*)buf.p;
-        return DR_OK;
-    };
+    auto set_moduli = [&](SieveArgs& m, int B, DevBuf& buf) { return set_sieve_moduli(c, pr, B, m, buf); };
     if ((rc = set_moduli(a, a.S_sub, c->items))) return rc;
     a.primes = (const uint32_t*)c->primes.p;
     a.pinv = (const u64*)c->pinv.p;
@@ -387,6 +397,7 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     uint64_t sq_hits = 0;
     for (size_t i = (size_t)a.sqC_first; i < pr.size(); ++i) sq_hits += (uint64_t)u_total / ((uint64_t)pr[i] * pr[i]);
     a.sq_off = nullptr;
+    a.sq_seg0 = 0;
     a.sq_pos = nullptr;
     if (sq_hits > 0) {
         if ((rc = ensure(c, c->sq_cnt, (size_t)nseg * 8))) return rc;
@@ -402,6 +413,7 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     a.dM = (int16_t*)c->dM.p;
     a.planes = (ulonglong2*)c->planes.p;
     a.ckpt = (int32_t*)c->ckpt.p;
+    a.cword0 = 0;
     a.wheel = (uint4*)c->wheel.p;
     a.seg_sum = (int32_t*)c->seg_sum.p;
     a.dplanes = nullptr;
@@ -431,12 +443,13 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     if (a.sq_off) {
         CU(cudaMemsetAsync(c->sq_cnt.p, 0, (size_t)nseg * 8, c->stream));
         CU(cudaMemsetAsync(c->sq_cur.p, 0, (size_t)nseg * 8, c->stream));
-        launch_sq_bucket_count((const uint32_t*)c->primes.p, a.sqC_first, (int)pr.size(), u_total, u_dense, dense_segs,
-                               lgS, (u64*)c->sq_cnt.p, c->stream);
+        launch_sq_bucket_count((const uint32_t*)c->primes.p, a.sqC_first, (int)pr.size(), 0, u_total, u_dense,
+                               dense_segs, lgS, 0, (u64*)c->sq_cnt.p, c->stream);
         launch_scan_u64((const u64*)c->sq_cnt.p, (u64*)c->sq_off.p, (u64)nseg, (u64*)c->sq_tmp.p,
                         scan_u64_tmp_elems((u64)nseg), c->stream);
-        launch_sq_bucket_fill((const uint32_t*)c->primes.p, a.sqC_first, (int)pr.size(), u_total, u_dense, dense_segs,
-                              lgS, (const u64*)c->sq_off.p, (u64*)c->sq_cur.p, (uint32_t*)c->sq_pos.p, c->stream);
+        launch_sq_bucket_fill((const uint32_t*)c->primes.p, a.sqC_first, (int)pr.size(), 0, u_total, u_dense,
+                              dense_segs, lgS, 0, (const u64*)c->sq_off.p, (u64*)c->sq_cur.p, (uint32_t*)c->sq_pos.p,
+                              c->stream);
         CU(cudaGetLastError());
         launches += 5;
     }
@@ -605,8 +618,202 @@ std::vector<S1WinItem> s1win_items(const QueryDev& q, int qi) {
 
 // Enqueue planning and sums for a batch of queries on the current table.
 // Only stream operations: it can run under graph capture.
+// A single query whose table (u_total values) exceeds the context's resident limit:
+// the table holds [1, u_res] (the dense tier and the first compressed segments); the
+// compressed segments above are sieved band by band, band_segs segments at a time, into
+// bplanes / bckpt, and after each band a planning pass and a sums pass take the S1
+// lookups whose quotient lies in that band (the idea of mertens_dr_windowed.hpp:218-374,
+// which streams M windows instead of storing M up to u).  The layout of the segments
+// and words is that of the whole table, so the segment scan continues across bands.
+struct StreamPlan {
+    int64_t u_total = 0, u_dense = 0, mu_limit = 0, u_res = 0;
+    int S = 0, block = 0;
+    int64_t dense_segs = 0, nseg = 0, nseg_res = 0, band_segs = 0, nbands = 0;
+    std::vector<uint64_t> band_sq;  // bucketed square hits of each band
+    int sqC_first = 0;
+};
+
+int64_t band_first_seg(const StreamPlan& sp, int64_t b) { return sp.nseg_res + b * sp.band_segs; }
+
+// Values (vlo, vhi] of band b.
+void band_values_of(const StreamPlan& sp, int64_t b, int64_t* vlo, int64_t* vhi) {
+    const int64_t c0 = band_first_seg(sp, b), c1 = std::min(sp.nseg, c0 + sp.band_segs);
+    *vlo = sp.u_dense + (c0 - sp.dense_segs) * sp.S;
+    *vhi = std::min(sp.u_total, sp.u_dense + (c1 - sp.dense_segs) * sp.S);
+}
+
+// Decide whether the query streams, and reserve every buffer the bands use before the
+// resident build (nothing may grow once launches are queued: the segment offsets of the
+// resident table carry into the first band).  *sp.nbands == 0: no streaming.
+int plan_stream(dr_ctx* c, int64_t X, int64_t ut, int64_t ud, int64_t ml, const dr_params& tune, StreamPlan* sp) {
+    *sp = StreamPlan{};
+    if (c->u_resident <= 0 || ut <= c->u_resident) return DR_OK;
+    if (X <= ut) return fail(DR_ERR_PARAMS, "a streamed table needs X > u_total (X = %lld, u_total = %lld)",
+                             (long long)X, (long long)ut);
+    sp->S = pick_segment(&tune);
+    const int64_t S = sp->S;
+    sp->block = tune.block_threads ? tune.block_threads : 1024;
+    sp->u_total = ut;
+    sp->u_dense = ud;
+    sp->mu_limit = ml;
+    // the resident part ends on a segment boundary of the whole table's layout
+    const int64_t res_segs = std::max<int64_t>(1, (c->u_resident - ud) / S);
+    sp->u_res = ud + res_segs * S;
+    if (sp->u_res >= ut) {
+        *sp = StreamPlan{};
+        return DR_OK;
+    }
+    if (ml > sp->u_res) return fail(DR_ERR_PARAMS, "mu_limit %lld above the resident table", (long long)ml);
+    sp->dense_segs = (ud + S - 1) / S;
+    sp->nseg = sp->dense_segs + (ut - ud + S - 1) / S;
+    sp->nseg_res = sp->dense_segs + res_segs;
+    sp->band_segs = c->band_values > 0 ? std::max<int64_t>(1, c->band_values / S) : res_segs;
+    sp->band_segs = std::min(sp->band_segs, sp->nseg - sp->nseg_res);
+    sp->nbands = (sp->nseg - sp->nseg_res + sp->band_segs - 1) / sp->band_segs;
+    const std::vector<uint32_t>& pr = primes_upto(c, isqrt_i64(ut));
+    // squares above S go to per-band buckets (the resident build buckets its own)
+    int k = 0;
+    while (k < (int)pr.size() && (uint64_t)pr[k] * pr[k] <= (uint64_t)S) ++k;
+    sp->sqC_first = k;
+    sp->band_sq.assign((size_t)sp->nbands, 0);
+    uint64_t max_sq = 0;
+    for (int64_t b = 0; b < sp->nbands; ++b) {
+        int64_t vlo, vhi;
+        band_values_of(*sp, b, &vlo, &vhi);
+        uint64_t h = 0;
+        for (size_t i = (size_t)k; i < pr.size(); ++i) {
+            const uint64_t q = (uint64_t)pr[i] * pr[i];
+            h += (uint64_t)vhi / q - (uint64_t)vlo / q;
+        }
+        sp->band_sq[(size_t)b] = h;
+        max_sq = std::max(max_sq, h);
+    }
+    const size_t bwords = (size_t)sp->band_segs * (size_t)(S / 64);
+    const size_t np = pr.size();
+    const size_t bsegs = (size_t)std::max(sp->band_segs, sp->nseg_res);
+    int rc;
+    if ((rc = ensure(c, c->seg_sum, (size_t)sp->nseg * 4))) return rc;
+    if ((rc = ensure(c, c->seg_off, (size_t)(sp->nseg + 1) * 4))) return rc;
+    if ((rc = ensure(c, c->primes, np * 4))) return rc;
+    if ((rc = ensure(c, c->pinv, np * 16))) return rc;
+    if ((rc = ensure(c, c->prcp, np * 8))) return rc;
+    if ((rc = ensure(c, c->items, (size_t)kMaxSieveItems * 16))) return rc;
+    if ((rc = ensure(c, c->bplanes, bwords * 16))) return rc;
+    if ((rc = ensure(c, c->bckpt, bwords * 4))) return rc;
+    if (max_sq > 0) {
+        if ((rc = ensure(c, c->sq_cnt, bsegs * 8))) return rc;
+        if ((rc = ensure(c, c->sq_cur, bsegs * 8))) return rc;
+        if ((rc = ensure(c, c->sq_off, (bsegs + 1) * 8))) return rc;
+        if ((rc = ensure(c, c->sq_tmp, scan_u64_tmp_elems((u64)bsegs) * 8))) return rc;
+        if ((rc = ensure(c, c->sq_pos, (size_t)max_sq * 4))) return rc;
+    }
+    return DR_OK;
+}
+
+// The band passes of a streamed table, after the resident sums pass on the same stream:
+// per band the square buckets, one full-mode sieve launch over its segments, the segment
+// scan (continuing from the segments before) and fix-up, then planning (S1 lookups with q
+// in the band only) and the sums kernel on the band's view of the table.
+int stream_bands(dr_ctx* c, const StreamPlan& sp, const SumsArgs& base, int grid, int* launches) {
+    const std::vector<uint32_t>& pr = primes_upto(c, isqrt_i64(sp.u_total));
+    const size_t np = pr.size();
+    std::vector<double> prcp(np);
+    for (size_t i = 0; i < np; ++i) prcp[i] = 1.0 / (double)pr[i];  // IEEE: RN(1/p)
+    const void* sp_ = stage_put(c, pr.data(), np * 4);
+    const void* sv = stage_put(c, c->host_pinv.data(), np * 16);
+    const void* sr = stage_put(c, prcp.data(), np * 8);
+    if (!sp_ || !sv || !sr) return fail(DR_ERR_NOMEM, "internal: staging area too small");
+    CU(cudaMemcpyAsync(c->primes.p, sp_, np * 4, cudaMemcpyHostToDevice, c->stream));
+    CU(cudaMemcpyAsync(c->pinv.p, sv, np * 16, cudaMemcpyHostToDevice, c->stream));
+    CU(cudaMemcpyAsync(c->prcp.p, sr, np * 8, cudaMemcpyHostToDevice, c->stream));
+    const int S = sp.S;
+    int lgS = 0;
+    while ((1 << lgS) < S) ++lgS;
+    SieveArgs a;
+    a.u_total = sp.u_total;
+    a.u_dense = sp.u_dense;
+    a.mu_limit = sp.mu_limit;
+    a.dense_segs = sp.dense_segs;
+    a.nseg = sp.nseg;
+    a.S = S;
+    a.S_sub = std::min(S, kSieveFullPass);
+    a.n_primes = (int)np;
+    a.sq_first = (int)(std::lower_bound(pr.begin(), pr.end(), 5u) - pr.begin());
+    a.w_first = (int)(std::lower_bound(pr.begin(), pr.end(), 13u) - pr.begin());
+    int rc = set_sieve_moduli(c, pr, a.S_sub, a, c->items);
+    if (rc) return rc;
+    a.primes = (const uint32_t*)c->primes.p;
+    a.pinv = (const u64*)c->pinv.p;
+    a.sqinv = (const u64*)c->pinv.p + np;
+    a.prcp = (const double*)c->prcp.p;
+    const int sqC = std::max(sp.sqC_first, a.sqB_first);  // squares above S: bucketed per band
+    a.sq_off = nullptr;
+    a.sq_seg0 = 0;
+    a.sq_pos = nullptr;
+    a.stencil4 = (const uint32_t*)c->stencil.p;
+    a.stencil_odd4 = (const uint32_t*)c->stencil_odd.p;
+    a.dplanes = nullptr;
+    a.dM = (int16_t*)c->dM.p;
+    a.planes = (ulonglong2*)c->bplanes.p;
+    a.ckpt = (int32_t*)c->bckpt.p;
+    a.wheel = (uint4*)c->wheel.p;
+    a.seg_sum = (int32_t*)c->seg_sum.p;
+    const size_t smem = sieve_smem_bytes(S, false);
+    int per = 0;
+    sieve_kernel_attrs(smem, false, sp.block, &per);
+    const int64_t sgrid = (int64_t)c->sm_count * std::max(per, 1);
+    const int64_t nwords_all = (sp.u_total - sp.u_dense + 63) / 64;
+    for (int64_t b = 0; b < sp.nbands; ++b) {
+        const int64_t c0 = band_first_seg(sp, b), c1 = std::min(sp.nseg, c0 + sp.band_segs);
+        int64_t vlo, vhi;
+        band_values_of(sp, b, &vlo, &vhi);
+        const int64_t cword0 = (c0 - sp.dense_segs) * (S / 64);
+        a.seg_begin = c0;
+        a.seg_end = c1;
+        a.cword0 = cword0;
+        a.sq_off = nullptr;
+        a.sq_pos = nullptr;
+        a.sq_seg0 = c0;
+        a.sqC_first = sqC;
+        if (sp.band_sq[(size_t)b] > 0 && sqC < (int)np) {
+            const u64 nb = (u64)(c1 - c0);
+            CU(cudaMemsetAsync(c->sq_cnt.p, 0, nb * 8, c->stream));
+            CU(cudaMemsetAsync(c->sq_cur.p, 0, nb * 8, c->stream));
+            launch_sq_bucket_count(a.primes, a.sqC_first, (int)np, vlo, vhi, sp.u_dense, sp.dense_segs, lgS, c0,
+                                   (u64*)c->sq_cnt.p, c->stream);
+            launch_scan_u64((const u64*)c->sq_cnt.p, (u64*)c->sq_off.p, nb, (u64*)c->sq_tmp.p,
+                            scan_u64_tmp_elems(nb), c->stream);
+            launch_sq_bucket_fill(a.primes, a.sqC_first, (int)np, vlo, vhi, sp.u_dense, sp.dense_segs, lgS, c0,
+                                  (const u64*)c->sq_off.p, (u64*)c->sq_cur.p, (uint32_t*)c->sq_pos.p, c->stream);
+            a.sq_off = (const u64*)c->sq_off.p;
+            a.sq_pos = (const uint32_t*)c->sq_pos.p;
+            *launches += 5;
+        } else {
+            a.sqC_first = (int)np;  // no bucketed hit in this band: squares thread-per-prime
+        }
+        launch_sieve(a, false, (int)std::max<int64_t>(1, std::min<int64_t>(c1 - c0, sgrid)), sp.block, smem, c->stream);
+        launch_seg_scan_range((const int32_t*)c->seg_sum.p, (int32_t*)c->seg_off.p, c0, c1, 1024, c->stream);
+        launch_fixup_range((int16_t*)c->dM.p, sp.u_dense, S, (const int32_t*)c->seg_off.p, (int32_t*)c->bckpt.p,
+                           nwords_all, sp.dense_segs, c0, c1, c->sm_count * 16, c->stream, cword0);
+        CU(cudaGetLastError());
+        SumsArgs sa = base;
+        sa.T.planes = (const ulonglong2*)c->bplanes.p;
+        sa.T.ckpt = (const int32_t*)c->bckpt.p;
+        sa.T.cbase = cword0;
+        CU(cudaMemsetAsync(c->ticket.p, 0, 8, c->stream));  // the work-queue counter (not the error flag)
+        launch_plan(sa.queries, sa.nq, sa.T, sa.n_slots, (u64*)c->ops.p, sa.acc, (i64*)c->counts.p, nullptr,
+                    (SlotDesc*)c->slots.p, c->sm_count, c->stream, S1Band{(u64)vlo + 1, (u64)vhi, 1});
+        launch_scan_u64((const u64*)c->ops.p, (u64*)c->prefix.p, sa.n_slots, (u64*)c->scan_tmp.p,
+                        scan_u64_tmp_elems(sa.n_slots), c->stream);
+        launch_sums(sa, grid, 256, c->stream);
+        CU(cudaGetLastError());
+        *launches += 9;
+    }
+    return DR_OK;
+}
+
 int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq, const dr_params* tuning,
-                    int* launches_out) {
+                    int* launches_out, const StreamPlan* sp = nullptr) {
     int rc;
     std::vector<QueryDev> qs((size_t)nq);
     u64 slots = 0;
@@ -635,7 +842,7 @@ int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq,
         q.win = q.win_max = 0;
         // opt-in: since the S1 terms that cancel between a candidate's two evaluations
         // are left out, the direct S1 is faster at every X measured (10^15 .. 10^18)
-        if (P[i].s1_window_log2 <= 0) continue;
+        if (P[i].s1_window_log2 <= 0 || sp) continue;
         const int wl = P[i].s1_window_log2;
         if (nq != 1 || q.N <= 0 || wl < 12 || wl > 16) continue;
         const int64_t W = int64_t(1) << wl;
@@ -701,8 +908,10 @@ int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq,
     if (slots > 0) {
         launch_inverse((double*)c->inv.p, inv_limit, (double2*)c->invw.p, invw_count, T.wheel, c->sm_count,
                        c->stream);
+        // a streamed table: this pass takes the S1 lookups with q <= u_res, the bands the rest
         launch_plan((const QueryDev*)c->queries.p, qn, T, slots, (u64*)c->ops.p, (u64*)c->acc.p, (i64*)c->counts.p,
-                    sw ? (S1WinDesc*)c->wdesc.p : nullptr, (SlotDesc*)c->slots.p, c->sm_count, c->stream);
+                    sw ? (S1WinDesc*)c->wdesc.p : nullptr, (SlotDesc*)c->slots.p, c->sm_count, c->stream,
+                    S1Band{0, sp ? (u64)sp->u_res : ~0ull, 0});
         launch_scan_u64((const u64*)c->ops.p, (u64*)c->prefix.p, slots, (u64*)c->scan_tmp.p,
                         scan_u64_tmp_elems(slots), c->stream);
         launches += 5;
@@ -744,6 +953,10 @@ int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq,
         launch_sums(sa, grid, 256, c->stream);
         CU(cudaGetLastError());
         launches += 1;
+        if (sp && sp->nbands > 0) {
+            rc = stream_bands(c, *sp, sa, grid, &launches);
+            if (rc) return rc;
+        }
     }
     CU(record_event(c, 4));
     CU(cudaMemcpyAsync(c->pinned, c->acc.p, (size_t)nq * 3 * 8, cudaMemcpyDeviceToHost, c->stream));
@@ -934,7 +1147,7 @@ int dr_ctx_destroy(dr_ctx* c) {
     DevBuf* bufs[] = {&c->dM, &c->planes, &c->ckpt, &c->wheel, &c->seg_sum, &c->seg_off, &c->primes, &c->pinv, &c->items, &c->stencil,
                       &c->queries, &c->ops, &c->prefix, &c->scan_tmp, &c->acc, &c->counts, &c->ticket, &c->misc,
                       &c->inv, &c->invw, &c->wdesc, &c->witems, &c->slots, &c->prcp, &c->sq_cnt, &c->sq_off, &c->sq_cur,
-                      &c->sq_pos, &c->sq_tmp, &c->items_odd, &c->stencil_odd, &c->dplanes};
+                      &c->sq_pos, &c->sq_tmp, &c->items_odd, &c->stencil_odd, &c->dplanes, &c->bplanes, &c->bckpt};
     for (DevBuf* b : bufs) release(c, *b);
     drop_graphs(c);
     if (c->pinned) cudaFreeHost(c->pinned);
@@ -951,6 +1164,14 @@ int dr_ctx_destroy(dr_ctx* c) {
     if (c->join) cudaEventDestroy(c->join);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
+    return DR_OK;
+}
+
+int dr_ctx_set_resident_limit(dr_ctx* c, int64_t u_resident, int64_t band_values) {
+    if (!c) return fail(DR_ERR_ARG, "ctx is NULL");
+    if (u_resident < 0 || band_values < 0) return fail(DR_ERR_ARG, "u_resident and band_values must be >= 0");
+    c->u_resident = u_resident;
+    c->band_values = band_values;
     return DR_OK;
 }
 
@@ -1128,9 +1349,15 @@ int dr_mertens_batch(dr_ctx* c, const int64_t* X, int64_t count, const dr_params
         if (attempt == 1 && !(rc == DR_ERR_NOMEM && release_scratch(c))) break;
         if (st) std::memset(st, 0, sizeof(*st));
         launches = 0;
-        rc = stage_reserve(c, stage_bytes_for(n_primes, count));
-        if (!rc) rc = build_table(c, ut, ud, ml, &tune, st);
-        if (!rc) rc = enqueue_queries(c, X, P.data(), count, &tune, &launches);
+        // a single query above the resident limit streams its table (plan_stream
+        // reserves the bands' buffers first; the resident build then covers [1, u_res])
+        StreamPlan sp;
+        rc = count == 1 ? plan_stream(c, X[0], ut, ud, ml, tune, &sp) : DR_OK;
+        const bool streamed = sp.nbands > 0;
+        const size_t n_res = streamed ? primes_upto(c, isqrt_i64(sp.u_res)).size() : 0;
+        if (!rc) rc = stage_reserve(c, stage_bytes_for(n_primes + n_res, count) + (streamed ? kMaxSieveItems * 16 : 0));
+        if (!rc) rc = build_table(c, streamed ? sp.u_res : ut, ud, ml, &tune, st);
+        if (!rc) rc = enqueue_queries(c, X, P.data(), count, &tune, &launches, streamed ? &sp : nullptr);
         if (!rc) break;
     }
     if (rc) return rc;

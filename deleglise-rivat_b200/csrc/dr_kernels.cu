@@ -447,9 +447,9 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
                 atomicOr(&buf32[j >> 2], 0x80u << ((j & 3) * 8));
         }
         if (a.sq_off) {
-            const u64 h1 = __ldg(a.sq_off + seg + 1);
+            const u64 h1 = __ldg(a.sq_off + (seg - a.sq_seg0) + 1);
             const uint32_t off = (uint32_t)(base - seg_base);  // this pass's first offset
-            for (u64 h = __ldg(a.sq_off + seg) + tid; h < h1; h += T) {
+            for (u64 h = __ldg(a.sq_off + (seg - a.sq_seg0)) + tid; h < h1; h += T) {
                 uint32_t j = __ldg(a.sq_pos + h);  // offset in the segment
                 if (j < off || j - off >= (uint32_t)len) continue;
                 j -= off;
@@ -584,7 +584,7 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
                 gs[w] = __popcll(nz) - 2 * __popcll(neg);
                 wpl[w] = make_ulonglong2(nz, neg);
                 if (dense) a.dplanes[(base >> 6) + w] = make_ulonglong2(nz, neg);
-                else a.planes[((base - a.u_dense) >> 6) + w] = make_ulonglong2(nz, neg);
+                else a.planes[((base - a.u_dense) >> 6) - a.cword0 + w] = make_ulonglong2(nz, neg);
             }
             __syncthreads();
             total = block_excl_scan(gs, nwords, wtot);
@@ -618,7 +618,7 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
                     }
                 }
             } else {
-                int32_t* ck = a.ckpt + ((base - a.u_dense) >> 6);
+                int32_t* ck = a.ckpt + (((base - a.u_dense) >> 6) - a.cword0);
                 for (int w = tid; w < nwords; w += T) ck[w] = carry + gs[w];
             }
         } else {
@@ -671,7 +671,7 @@ __global__ void __launch_bounds__(1024) sieve_kernel(const SieveArgs a) {
                     if (dense) {
                         a.dplanes[(base >> 6) + w] = make_ulonglong2(nz, neg);
                     } else {
-                        const i64 wbase = (base - a.u_dense) >> 6;
+                        const i64 wbase = ((base - a.u_dense) >> 6) - a.cword0;
                         a.planes[wbase + w] = make_ulonglong2(nz, neg);
                         a.ckpt[wbase + w] = carry + gs[4 * w];
                     }
@@ -836,37 +836,44 @@ __device__ __forceinline__ void segment_of(u64 n, i64 u_dense, i64 dense_segs, i
 }
 
 // one CTA per prime, threads over the multiples m*p^2
-__global__ void sq_bucket_count_kernel(const uint32_t* primes, int first, i64 u_total, i64 u_dense, i64 dense_segs,
-                                       int lgS, u64* counts) {
+// The multiples of p^2 in (vlo, vhi]; bucket arrays indexed by segment - seg0 (a
+// streamed band buckets only its own segments: vlo, seg0 = its first value - 1 and
+// segment; the whole table: vlo = seg0 = 0, vhi = u_total).
+__global__ void sq_bucket_count_kernel(const uint32_t* primes, int first, i64 vlo, i64 vhi, i64 u_dense,
+                                       i64 dense_segs, int lgS, i64 seg0, u64* counts) {
     const u64 p = primes[first + blockIdx.x], sq = p * p;
-    for (u64 n = sq * (threadIdx.x + 1); n <= (u64)u_total; n += sq * blockDim.x) {
+    for (u64 n = sq * ((u64)vlo / sq + 1 + threadIdx.x); n <= (u64)vhi; n += sq * blockDim.x) {
         u64 seg;
         uint32_t j;
         segment_of(n, u_dense, dense_segs, lgS, &seg, &j);
-        atomicAdd(counts + seg, 1ull);
+        atomicAdd(counts + (seg - (u64)seg0), 1ull);
     }
 }
 
-__global__ void sq_bucket_fill_kernel(const uint32_t* primes, int first, i64 u_total, i64 u_dense, i64 dense_segs,
-                                      int lgS, const u64* off, u64* cur, uint32_t* pos) {
+__global__ void sq_bucket_fill_kernel(const uint32_t* primes, int first, i64 vlo, i64 vhi, i64 u_dense,
+                                      i64 dense_segs, int lgS, i64 seg0, const u64* off, u64* cur, uint32_t* pos) {
     const u64 p = primes[first + blockIdx.x], sq = p * p;
-    for (u64 n = sq * (threadIdx.x + 1); n <= (u64)u_total; n += sq * blockDim.x) {
+    for (u64 n = sq * ((u64)vlo / sq + 1 + threadIdx.x); n <= (u64)vhi; n += sq * blockDim.x) {
         u64 seg;
         uint32_t j;
         segment_of(n, u_dense, dense_segs, lgS, &seg, &j);
-        pos[off[seg] + atomicAdd(cur + seg, 1ull)] = j;
+        const u64 b = seg - (u64)seg0;
+        pos[off[b] + atomicAdd(cur + b, 1ull)] = j;
     }
 }
 
-void launch_sq_bucket_count(const uint32_t* primes, int first, int n, i64 u_total, i64 u_dense, i64 dense_segs,
-                            int lgS, u64* counts, cudaStream_t s) {
-    if (n > first) sq_bucket_count_kernel<<<n - first, 128, 0, s>>>(primes, first, u_total, u_dense, dense_segs, lgS, counts);
-}
-
-void launch_sq_bucket_fill(const uint32_t* primes, int first, int n, i64 u_total, i64 u_dense, i64 dense_segs,
-                           int lgS, const u64* off, u64* cur, uint32_t* pos, cudaStream_t s) {
+void launch_sq_bucket_count(const uint32_t* primes, int first, int n, i64 vlo, i64 vhi, i64 u_dense, i64 dense_segs,
+                            int lgS, i64 seg0, u64* counts, cudaStream_t s) {
     if (n > first)
-        sq_bucket_fill_kernel<<<n - first, 128, 0, s>>>(primes, first, u_total, u_dense, dense_segs, lgS, off, cur, pos);
+        sq_bucket_count_kernel<<<n - first, 128, 0, s>>>(primes, first, vlo, vhi, u_dense, dense_segs, lgS, seg0,
+                                                         counts);
+}
+
+void launch_sq_bucket_fill(const uint32_t* primes, int first, int n, i64 vlo, i64 vhi, i64 u_dense, i64 dense_segs,
+                           int lgS, i64 seg0, const u64* off, u64* cur, uint32_t* pos, cudaStream_t s) {
+    if (n > first)
+        sq_bucket_fill_kernel<<<n - first, 128, 0, s>>>(primes, first, vlo, vhi, u_dense, dense_segs, lgS, seg0, off,
+                                                        cur, pos);
 }
 
 // ---------------------------------------------------------------------------
@@ -903,7 +910,7 @@ void launch_seg_scan_range(const int32_t* in, int32_t* out, i64 b0, i64 b1, int 
 // and to the checkpoints [w0, w1) (int16 wrap-around on the dense tier, as the
 // reference's int16 conversion).
 __global__ void fixup_kernel(int16_t* dM, i64 u_dense, int lgS, const int32_t* seg_off, int32_t* ckpt, i64 g0,
-                             i64 g1, i64 w0, i64 w1, i64 dense_segs) {
+                             i64 g1, i64 w0, i64 w1, i64 dense_segs, i64 cword0) {
     const i64 stride = (i64)gridDim.x * blockDim.x;
     const i64 t0 = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     for (i64 i = g0 + t0; i < g1; i += stride) {
@@ -921,12 +928,12 @@ __global__ void fixup_kernel(int16_t* dM, i64 u_dense, int lgS, const int32_t* s
             for (i64 k = 8 * i; k < u_dense; ++k) dM[k] = (int16_t)(dM[k] + off);
         }
     }
-    for (i64 w = w0 + t0; w < w1; w += stride) ckpt[w] += seg_off[dense_segs + ((64 * w) >> lgS)];
+    for (i64 w = w0 + t0; w < w1; w += stride) ckpt[w - cword0] += seg_off[dense_segs + ((64 * w) >> lgS)];
 }
 
 // The fix-up of segments [b0, b1): their dense groups and their checkpoint words.
 void launch_fixup_range(int16_t* dM, i64 u_dense, int S, const int32_t* seg_off, int32_t* ckpt, i64 nwords,
-                        i64 dense_segs, i64 b0, i64 b1, int blocks, cudaStream_t s) {
+                        i64 dense_segs, i64 b0, i64 b1, int blocks, cudaStream_t s, i64 cword0) {
     int lgS = 0;  // S is a power of two (2^12 .. 2^18)
     while ((1 << lgS) < S) ++lgS;
     const i64 n8 = (u_dense + 7) / 8;
@@ -938,14 +945,14 @@ void launch_fixup_range(int16_t* dM, i64 u_dense, int S, const int32_t* seg_off,
     const i64 work = std::max(g1x - g0, w1 - w0);
     if (work <= 0) return;
     const int grid = (int)std::max<i64>(1, std::min<i64>((work + 255) / 256, (i64)blocks));
-    fixup_kernel<<<grid, 256, 0, s>>>(dM, u_dense, lgS, seg_off, ckpt, g0, g1x, w0, w1, dense_segs);
+    fixup_kernel<<<grid, 256, 0, s>>>(dM, u_dense, lgS, seg_off, ckpt, g0, g1x, w0, w1, dense_segs, cword0);
 }
 
 void launch_fixup(int16_t* dM, i64 u_dense, int S, const int32_t* seg_off, int32_t* ckpt, i64 nwords,
                   i64 dense_segs, int sm_count, cudaStream_t s) {
     const i64 nseg_all = dense_segs + (nwords * 64 + S - 1) / S;
     launch_fixup_range(dM, u_dense, S, seg_off, ckpt, nwords, dense_segs, 0, std::max<i64>(nseg_all, dense_segs),
-                       sm_count * 8, s);
+                       sm_count * 8, s, 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -980,9 +987,11 @@ __device__ __forceinline__ u64 s1_compressed_lookups(const EvalDesc& d, const Ta
 
 // counts[kCountsPerQuery*q + 0..4]: terms, evaluations, S1 lookups, S2 wheel
 // positions, compressed-tier S1 lookups -- summed over the warp before the atomics
+// (a band pass of a streamed table, band.s1_only, counts only its S1 lookups and adds
+// no constant part: those belong to the resident pass)
 __global__ void plan_kernel(const QueryDev* __restrict__ qs, int nq, const TableView T, u64 n_slots,
                             u64* __restrict__ ops, u64* __restrict__ acc, i64* __restrict__ counts,
-                            S1WinDesc* __restrict__ wdesc, SlotDesc* __restrict__ slots) {
+                            S1WinDesc* __restrict__ wdesc, SlotDesc* __restrict__ slots, const S1Band band) {
     // whole warps step together (the stride is a multiple of 32), so the counters
     // can be summed over the warp with every lane taking part
     const u64 stride = (u64)gridDim.x * blockDim.x;
@@ -996,7 +1005,7 @@ __global__ void plan_kernel(const QueryDev* __restrict__ qs, int nq, const Table
             const QueryDev Q = qs[qi];
             const u64 local = s - Q.slot_base;
             EvalDesc d;
-            decode_eval(Q, T, (i64)(local >> 1), (int)(local & 1), d);
+            decode_eval(Q, T, (i64)(local >> 1), (int)(local & 1), d, band);
             ops[s] = d.total;
             pack_slot(d, slots + s);
             if (wdesc && Q.win) {
@@ -1015,9 +1024,11 @@ __global__ void plan_kernel(const QueryDev* __restrict__ qs, int nq, const Table
                 wdesc[s] = w;
             }
             if (d.kind != EVAL_NONE) {
-                v[0] = (u64)(d.coef * eval_constant(d, T));
-                v[1] = (local & 1) == 0 ? 1 : 0;
-                v[2] = 1;
+                if (!band.s1_only) {
+                    v[0] = (u64)(d.coef * eval_constant(d, T));
+                    v[1] = (local & 1) == 0 ? 1 : 0;
+                    v[2] = 1;
+                }
                 u64 s1d = 0, s1f = 0;  // lookups left to the sums kernel, all lookups
                 for (int g = 0; g < kS1Seg; ++g) {
                     s1d += (u64)d.s1_cnt[g];
@@ -1049,10 +1060,10 @@ __global__ void plan_kernel(const QueryDev* __restrict__ qs, int nq, const Table
 }
 
 void launch_plan(const QueryDev* q, int nq, const TableView& T, u64 n_slots, u64* ops, u64* acc, i64* counts,
-                 S1WinDesc* wdesc, SlotDesc* slots, int sm_count, cudaStream_t s) {
+                 S1WinDesc* wdesc, SlotDesc* slots, int sm_count, cudaStream_t s, const S1Band& band) {
     if (n_slots == 0) return;
     const int grid = (int)std::min<u64>((n_slots + 127) / 128, (u64)sm_count * 16);
-    plan_kernel<<<grid, 128, 0, s>>>(q, nq, T, n_slots, ops, acc, counts, wdesc, slots);
+    plan_kernel<<<grid, 128, 0, s>>>(q, nq, T, n_slots, ops, acc, counts, wdesc, slots, band);
 }
 
 // Direct answers for queries with X <= table u_total (get_M, :1465-1467).

@@ -44,7 +44,8 @@ struct SieveArgs {
     const u64* sqinv;          // floor((2^64-1)/p^2) per prime
     const double* prcp;        // RN(1/p) per prime (32-bit offset route; NULL: umod_inv only)
     int sqC_first;             // first prime whose square is bucketed (p^2 > S); n_primes: none
-    const u64* sq_off;         // [nseg + 1]: bucketed square hits of each segment (NULL: no bucket)
+    const u64* sq_off;         // bucketed square hits of each segment from sq_seg0 on (NULL: no bucket)
+    i64 sq_seg0;               // segment of sq_off[0] (0, or a streamed band's first segment)
     const uint32_t* sq_pos;    // their positions within the segment
     const uint32_t* stencil4;  // 4 copies shifted by 0..3 bytes, kStencilWords each (full mode)
     const uint32_t* stencil_odd4;  // the same for the odd-value stencil, kStencilOddWords each
@@ -53,6 +54,8 @@ struct SieveArgs {
     int16_t* dM;
     ulonglong2* planes;
     int32_t* ckpt;
+    i64 cword0;                // compressed-tier word held in planes[0] / ckpt[0] (0, or a
+                               // streamed band's first word; such bands run in full mode)
     uint4* wheel;
     int32_t* seg_sum;
 };
@@ -102,13 +105,14 @@ struct SumsArgs {
 };
 
 void launch_sieve(const SieveArgs& a, bool odd, int grid, int block, size_t smem, cudaStream_t s);
-// Bucketed squares: the multiples m*p^2 <= u_total of the primes p = primes[first..n)
+// Bucketed squares: the multiples m*p^2 in (vlo, vhi] of the primes p = primes[first..n)
 // (p^2 > S: at most one per segment), counted per segment, then written per segment
-// in the order of off = exclusive scan of the counts (cur: zeroed cursors).
-void launch_sq_bucket_count(const uint32_t* primes, int first, int n, i64 u_total, i64 u_dense, i64 dense_segs,
-                            int lgS, u64* counts, cudaStream_t s);
-void launch_sq_bucket_fill(const uint32_t* primes, int first, int n, i64 u_total, i64 u_dense, i64 dense_segs,
-                           int lgS, const u64* off, u64* cur, uint32_t* pos, cudaStream_t s);
+// in the order of off = exclusive scan of the counts (cur: zeroed cursors); bucket
+// arrays indexed by segment - seg0 (the whole table: vlo = seg0 = 0, vhi = u_total).
+void launch_sq_bucket_count(const uint32_t* primes, int first, int n, i64 vlo, i64 vhi, i64 u_dense, i64 dense_segs,
+                            int lgS, i64 seg0, u64* counts, cudaStream_t s);
+void launch_sq_bucket_fill(const uint32_t* primes, int first, int n, i64 vlo, i64 vhi, i64 u_dense, i64 dense_segs,
+                           int lgS, i64 seg0, const u64* off, u64* cur, uint32_t* pos, cudaStream_t s);
 
 // Moduli with at least kItemDiv hits in the B bytes a segment sieves (m < B/kItemDiv)
 // are marked by warp work items, larger ones one prime per thread (at most kItemDiv
@@ -139,8 +143,10 @@ void launch_seg_scan(const int32_t* in, int32_t* out, i64 n, cudaStream_t s);
 // 0 for b0 = 0); also writes out[b1].  One CTA of `threads` (32 .. 1024, a multiple of 32).
 void launch_seg_scan_range(const int32_t* in, int32_t* out, i64 b0, i64 b1, int threads, cudaStream_t s);
 // Offsets added to the dense prefix and the checkpoints of the segments [b0, b1).
+// cword0: the compressed-tier word held in ckpt[0] (0 for a whole table, a band's
+// first word for a streamed band)
 void launch_fixup_range(int16_t* dM, i64 u_dense, int S, const int32_t* seg_off, int32_t* ckpt, i64 nwords,
-                        i64 dense_segs, i64 b0, i64 b1, int blocks, cudaStream_t s);
+                        i64 dense_segs, i64 b0, i64 b1, int blocks, cudaStream_t s, i64 cword0 = 0);
 void launch_fixup(int16_t* dM, i64 u_dense, int S, const int32_t* seg_off, int32_t* ckpt, i64 nwords,
                   i64 dense_segs, int sm_count, cudaStream_t s);
 // Per-query counters written by plan_kernel: counts[kCountsPerQuery*q + 0..4] =
@@ -148,7 +154,8 @@ void launch_fixup(int16_t* dM, i64 u_dense, int S, const int32_t* seg_off, int32
 // whose quotient lies in the compressed tier (q > u_dense).
 constexpr int kCountsPerQuery = 5;
 void launch_plan(const QueryDev* q, int nq, const TableView& T, u64 n_slots, u64* ops, u64* acc,
-                 i64* counts, S1WinDesc* wdesc, SlotDesc* slots, int sm_count, cudaStream_t s);
+                 i64* counts, S1WinDesc* wdesc, SlotDesc* slots, int sm_count, cudaStream_t s,
+                 const S1Band& band = S1Band{0, ~0ull, 0});
 // Windowed S1 (window length win: a power of two, 2^12 .. 2^16).
 void launch_s1win(const S1WinArgs& a, u64 win, int sm_count, cudaStream_t s);
 void launch_scan_u64(const u64* in, u64* out, u64 n, u64* tmp, size_t tmp_elems, cudaStream_t s);

@@ -272,11 +272,13 @@ extern "C" int dr_table_build_noalloc(int device, void* stream, int64_t u_total,
         a.prcp = nullptr;  // offsets from the 64-bit reciprocals, squares without a bucket
         a.sqC_first = a.n_primes;
         a.sq_off = nullptr;
+        a.sq_seg0 = 0;
         a.sq_pos = nullptr;
         a.stencil4 = d.scratch + kOffStencil;
         a.dM = dM;
         a.planes = (ulonglong2*)planes;
         a.ckpt = ckpt;
+        a.cword0 = 0;
         a.wheel = (uint4*)wheel;
         a.seg_sum = (int32_t*)(d.scratch + kOffSegSum);
         int32_t* seg_off = (int32_t*)(d.scratch + kOffSegOff);

@@ -124,6 +124,7 @@ def lib():
             "dr_ctx_destroy": (i32, [vp]),
             "dr_last_error": (ctypes.c_char_p, []),
             "dr_ctx_set_hbm_budget": (i32, [vp, u64]),
+            "dr_ctx_set_resident_limit": (i32, [vp, i64, i64]),
             "dr_device_info": (i32, [i32, ctypes.POINTER(i32), ctypes.POINTER(u64)]),
             "dr_default_params": (i32, [i64, i32, P]),
             "dr_reference_gpu_params": (i32, [i64, i32, P]),
@@ -174,7 +175,8 @@ def exported_symbols() -> list:
     """Names of the C-ABI entry points this binding expects (for load tests)."""
     lib()
     return [
-        "dr_ctx_create", "dr_ctx_destroy", "dr_last_error", "dr_ctx_set_hbm_budget", "dr_device_info",
+        "dr_ctx_create", "dr_ctx_destroy", "dr_last_error", "dr_ctx_set_hbm_budget", "dr_ctx_set_resident_limit",
+        "dr_device_info",
         "dr_default_params", "dr_reference_gpu_params", "dr_check_params", "dr_table_bytes", "dr_query_bytes", "dr_mertens", "dr_mertens_batch",
         "dr_batch_checksums", "dr_table_build", "dr_table_read", "dr_table_read_wheel", "dr_table_checksums",
         "dr_debug_udiv", "dr_debug_udiv_rcp", "dr_debug_udiv32", "dr_debug_piece", "dr_debug_piece32",
@@ -277,6 +279,12 @@ class Engine:
 
     def set_hbm_budget(self, nbytes: int):
         _check(lib().dr_ctx_set_hbm_budget(self._ctx, int(nbytes)))
+
+    def set_resident_limit(self, u_resident: int, band_values: int = 0):
+        """Stream the compressed tier of single-query tables above u_resident values in
+        bands of band_values (0: the resident compressed tier's size); 0 holds every
+        table whole."""
+        _check(lib().dr_ctx_set_resident_limit(self._ctx, int(u_resident), int(band_values)))
 
     # --- reference-named entry points ---------------------------------------
     def compute_mertens(self, X: int, params: Optional[Params] = None) -> int:

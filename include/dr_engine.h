@@ -97,6 +97,18 @@ const char *dr_last_error(void);
  * would exceed the cap first releases them (after the work in flight) and runs once
  * more, so only a call that does not fit on its own fails with DR_ERR_NOMEM. */
 int dr_ctx_set_hbm_budget(dr_ctx *ctx, uint64_t bytes);
+/* Streamed table for tables larger than device memory (the idea of the reference's
+ * windowed engine, mertens_dr_windowed.hpp:218-374, which streams M windows over
+ * [1, u] instead of storing them).  A single query (dr_mertens) whose u_total
+ * exceeds u_resident keeps only M up to u_res (u_resident rounded down to a sieve
+ * segment of the compressed tier, at least one segment above u_dense) in memory; the
+ * compressed tier above is sieved band by band, band_values values at a time (0: as
+ * many as the resident compressed tier holds), and after each band the S1 lookups
+ * whose quotient falls in it are summed.  M(X) and the C/S1/S2 checksums are those
+ * of the whole table.  Needs X > u_total and mu_limit <= u_res; batches never
+ * stream.  u_resident = 0 (the default) holds every table whole.  The bands'
+ * build and lookups count in dr_stats.sums_ms. */
+int dr_ctx_set_resident_limit(dr_ctx *ctx, int64_t u_resident, int64_t band_values);
 int dr_device_info(int device, int *sm_count, uint64_t *hbm_bytes);
 
 /* Parameters ------------------------------------------------------------- */
