@@ -353,11 +353,11 @@ def run_engine(args, world, rank, local):
     default = dr_b200.default_params(X, dr_b200.POLICY_REFERENCE)
     if args.u:
         tuned = with_table_size(tuned, X, int(float(args.u)))
-    stream = None
+    streamed = None
     if args.resident:
         # streamed table: M held up to the resident limit, the rest sieved band by band
-        stream = {"u_resident": int(float(args.resident)), "band_values": int(float(args.band or 0))}
-        eng.set_resident_limit(stream["u_resident"], stream["band_values"])
+        streamed = {"u_resident": int(float(args.resident)), "band_values": int(float(args.band or 0))}
+        eng.set_resident_limit(streamed["u_resident"], streamed["band_values"])
 
     def check(m):
         if want is not None and m != want:
@@ -397,7 +397,7 @@ def run_engine(args, world, rank, local):
     sec_per, host_per, stats = timed(tuned, args.steps, clocks)
     value = sec_per / world  # whole job: N replicas finish N results in sec_per
 
-    if stream:
+    if streamed:
         eng.set_resident_limit(0)  # the comparison arms hold their tables whole
     # the plain path with the reference's default parameters, same run
     dsec = dhost = None
@@ -489,7 +489,7 @@ def run_engine(args, world, rank, local):
     issue_peak = sms * 4 * f_mhz * 1e6
     roofline = sums_roofline(s0_, sums, peak, peak_kind, issue_peak, f_mhz)
     # a streamed table's bands are built inside the sums phase: no table-phase roofline
-    table_roofline = None if stream else sieve_roofline(tuned, tab, peak, peaks_int, issue_peak, sms)
+    table_roofline = None if streamed else sieve_roofline(tuned, tab, peak, peaks_int, issue_peak, sms)
     line = {
         "metric": "sec per M(10^16)" if X == X_HEADLINE else f"sec per M({X})", "value": value, "unit": "s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_per * 1e3,
@@ -502,7 +502,7 @@ def run_engine(args, world, rank, local):
         "phases_ms": phases,
         "default_params": None if dsec is None else {"ms_per_step": dsec * 1e3, "u_total": default.u_total,
                                                      "cx": default.cx, "tuned_speedup": dsec / sec_per, "e2e_s": dhost},
-        "stream": stream,
+        "stream": streamed,
         "learned_tuner": learned,
         "gpu_launches": launches,
         "e2e": {"value": host_per / world, "unit": "s", "h2d_bytes_per_step": int(s0_.h2d_bytes),

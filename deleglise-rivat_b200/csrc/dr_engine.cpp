@@ -414,6 +414,7 @@ int build_table(dr_ctx* c, int64_t u_total, int64_t u_dense, int64_t mu_limit, c
     a.planes = (ulonglong2*)c->planes.p;
     a.ckpt = (int32_t*)c->ckpt.p;
     a.cword0 = 0;
+    a.hplanes = a.planes;
     a.wheel = (uint4*)c->wheel.p;
     a.seg_sum = (int32_t*)c->seg_sum.p;
     a.dplanes = nullptr;
@@ -698,6 +699,7 @@ int plan_stream(dr_ctx* c, int64_t X, int64_t ut, int64_t ud, int64_t ml, const 
     if ((rc = ensure(c, c->pinv, np * 16))) return rc;
     if ((rc = ensure(c, c->prcp, np * 8))) return rc;
     if ((rc = ensure(c, c->items, (size_t)kMaxSieveItems * 16))) return rc;
+    if ((rc = ensure(c, c->items_odd, (size_t)kMaxSieveItems * 16))) return rc;
     if ((rc = ensure(c, c->bplanes, bwords * 16))) return rc;
     if ((rc = ensure(c, c->bckpt, bwords * 4))) return rc;
     if (max_sq > 0) {
@@ -729,7 +731,8 @@ int stream_bands(dr_ctx* c, const StreamPlan& sp, const SumsArgs& base, int grid
     const int S = sp.S;
     int lgS = 0;
     while ((1 << lgS) < S) ++lgS;
-    SieveArgs a;
+    SieveArgs af;
+    SieveArgs& a = af;  // full-mode arguments
     a.u_total = sp.u_total;
     a.u_dense = sp.u_dense;
     a.mu_limit = sp.mu_limit;
@@ -756,18 +759,29 @@ int stream_bands(dr_ctx* c, const StreamPlan& sp, const SumsArgs& base, int grid
     a.dM = (int16_t*)c->dM.p;
     a.planes = (ulonglong2*)c->bplanes.p;
     a.ckpt = (int32_t*)c->bckpt.p;
+    a.hplanes = (const ulonglong2*)c->planes.p;  // the resident compressed tier
     a.wheel = (uint4*)c->wheel.p;
     a.seg_sum = (int32_t*)c->seg_sum.p;
-    const size_t smem = sieve_smem_bytes(S, false);
-    int per = 0;
+    const size_t smem = sieve_smem_bytes(S, false), smem_o = sieve_smem_bytes(S, true);
+    int per = 0, per_o = 0;
     sieve_kernel_attrs(smem, false, sp.block, &per);
+    sieve_kernel_attrs(smem_o, true, sp.block, &per_o);
     const int64_t sgrid = (int64_t)c->sm_count * std::max(per, 1);
+    const int64_t sgrid_o = (int64_t)c->sm_count * std::max(per_o, 1);
+    // A band whose halves n/2 all lie in the resident compressed tier (vlo >= 2 u_dense,
+    // vhi well below 2 u_res) runs in odd mode: its even values take mu from the resident
+    // plane words of their halves (odd mode needs u_dense on a 64-value word).
+    SieveArgs ao = a;
+    const bool odd_ok = sp.u_dense % 64 == 0;
+    if (odd_ok && (rc = set_sieve_moduli(c, pr, S / 2, ao, c->items_odd))) return rc;
     const int64_t nwords_all = (sp.u_total - sp.u_dense + 63) / 64;
     for (int64_t b = 0; b < sp.nbands; ++b) {
         const int64_t c0 = band_first_seg(sp, b), c1 = std::min(sp.nseg, c0 + sp.band_segs);
         int64_t vlo, vhi;
         band_values_of(sp, b, &vlo, &vhi);
         const int64_t cword0 = (c0 - sp.dense_segs) * (S / 64);
+        const bool odd = odd_ok && vlo >= 2 * sp.u_dense && vhi + 2 * (int64_t)S <= 2 * sp.u_res;
+        SieveArgs& a = odd ? ao : af;
         a.seg_begin = c0;
         a.seg_end = c1;
         a.cword0 = cword0;
@@ -791,7 +805,8 @@ int stream_bands(dr_ctx* c, const StreamPlan& sp, const SumsArgs& base, int grid
         } else {
             a.sqC_first = (int)np;  // no bucketed hit in this band: squares thread-per-prime
         }
-        launch_sieve(a, false, (int)std::max<int64_t>(1, std::min<int64_t>(c1 - c0, sgrid)), sp.block, smem, c->stream);
+        launch_sieve(a, odd, (int)std::max<int64_t>(1, std::min<int64_t>(c1 - c0, odd ? sgrid_o : sgrid)), sp.block,
+                     odd ? smem_o : smem, c->stream);
         launch_seg_scan_range((const int32_t*)c->seg_sum.p, (int32_t*)c->seg_off.p, c0, c1, 1024, c->stream);
         launch_fixup_range((int16_t*)c->dM.p, sp.u_dense, S, (const int32_t*)c->seg_off.p, (int32_t*)c->bckpt.p,
                            nwords_all, sp.dense_segs, c0, c1, c->sm_count * 16, c->stream, cword0);

@@ -245,7 +245,7 @@ __device__ __forceinline__ void planes_odd_mode(const SieveArgs& a, const uint32
     u64 g = ((u64)__funnelshift_l(gl, gh, sh) << 32) | __funnelshift_l(gh, gl, sh);
     const i64 q0 = (base >> 1) + 32 * (i64)w;  // 0-based bit index of m = q0 + 1
     const i64 G = q0 >> 6;
-    const ulonglong2 P = G < (a.u_dense >> 6) ? __ldg(a.dplanes + G) : __ldg(a.planes + (G - (a.u_dense >> 6)));
+    const ulonglong2 P = G < (a.u_dense >> 6) ? __ldg(a.dplanes + G) : __ldg(a.hplanes + (G - (a.u_dense >> 6)));
     const uint32_t hz = (uint32_t)(((q0 >> 5) & 1) ? P.x >> 32 : P.x);
     const uint32_t hg = (uint32_t)(((q0 >> 5) & 1) ? P.y >> 32 : P.y);
     z |= spread32(hz & 0x55555555u) << 1;

@@ -55,7 +55,10 @@ struct SieveArgs {
     ulonglong2* planes;
     int32_t* ckpt;
     i64 cword0;                // compressed-tier word held in planes[0] / ckpt[0] (0, or a
-                               // streamed band's first word; such bands run in full mode)
+                               // streamed band's first word)
+    const ulonglong2* hplanes; // the compressed tier's plane words from word 0, where odd mode
+                               // reads the halves (planes itself, or the resident table's
+                               // planes for a streamed band whose halves are resident)
     uint4* wheel;
     int32_t* seg_sum;
 };

@@ -279,6 +279,7 @@ extern "C" int dr_table_build_noalloc(int device, void* stream, int64_t u_total,
         a.planes = (ulonglong2*)planes;
         a.ckpt = ckpt;
         a.cword0 = 0;
+        a.hplanes = (const ulonglong2*)planes;
         a.wheel = (uint4*)wheel;
         a.seg_sum = (int32_t*)(d.scratch + kOffSegSum);
         int32_t* seg_off = (int32_t*)(d.scratch + kOffSegOff);

@@ -6,7 +6,9 @@ quotient falls in it are summed (the idea of mertens_dr_windowed.hpp:218-374, wh
 streams M windows over [1, u] instead of storing them).  Every lookup is the same term of
 the same sum, so M(X), the C/S1/S2 checksums and the op counts equal those of the whole
 table at the same parameters -- for every resident limit, band length and segment length,
-including bands of one segment and a last band that ends inside a segment.
+including bands of one segment, a last band that ends inside a segment, and bands sieved
+in odd mode (their halves n/2 in the resident table: 3e9 resident of M(10^15)'s 5.4e9)
+beside bands sieved in full mode.
 """
 import pytest
 
@@ -33,7 +35,8 @@ def test_streamed_matches_whole_table(streaming):
     cases = [
         (10**12, dr_b200.POLICY_COMPRESSED, 14, [(20000000, 1 << 16), (30000000, 0), (14000000, 5000000)], 62366),
         (10**13 + 7, dr_b200.POLICY_COMPRESSED, 16, [(10**8, 3 * 10**7), (5 * 10**7, 1)], None),
-        (10**15, dr_b200.POLICY_COMPRESSED, 18, [(10**9, 1 << 30), (6 * 10**8, 2 * 10**9)], -3216373),
+        (10**15, dr_b200.POLICY_COMPRESSED, 18, [(10**9, 1 << 30), (6 * 10**8, 2 * 10**9), (3 * 10**9, 10**9)],
+         -3216373),
         (10**15, dr_b200.POLICY_GPU, 17, [(2 * 10**9, 10**9)], -3216373),
     ]
     for X, policy, lg, splits, known in cases:
