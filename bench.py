@@ -481,6 +481,9 @@ def run_engine(args, world, rank, local):
     peak, peak_kind = load_peaks()
     s0_ = stats[0]
     phases = {"table_ms": tab, "plan_ms": plan, "sums_ms": sums}
+    if streamed:  # both within sums_ms
+        phases.update({"band_table_ms": statistics.mean(s.band_table_ms for s in stats),
+                       "band_sums_ms": statistics.mean(s.band_sums_ms for s in stats), "bands": stats[0].bands})
     clk = clocks.summary()
     sms = torch.cuda.get_device_properties(local).multi_processor_count
     # issue ceiling: 4 warp instructions per SM and clock at the median SM clock

@@ -75,6 +75,8 @@ struct dr_ctx {
     // is built and consumed band by band in these two buffers, never held whole
     DevBuf bplanes, bckpt;
     int64_t u_resident = 0, band_values = 0;
+    std::vector<cudaEvent_t> bev;  // band timing: start, then per band after its build and after its sums
+    int64_t last_bands = 0;        // bands the enqueued call streams
     // query buffers
     DevBuf queries, ops, prefix, scan_tmp, acc, counts, ticket, misc, inv, invw, wdesc, witems, slots;
     // table state
@@ -775,6 +777,13 @@ int stream_bands(dr_ctx* c, const StreamPlan& sp, const SumsArgs& base, int grid
     const bool odd_ok = sp.u_dense % 64 == 0;
     if (odd_ok && (rc = set_sieve_moduli(c, pr, S / 2, ao, c->items_odd))) return rc;
     const int64_t nwords_all = (sp.u_total - sp.u_dense + 63) / 64;
+    while ((int64_t)c->bev.size() < 2 * sp.nbands + 1) {
+        cudaEvent_t e;
+        CU(cudaEventCreate(&e));
+        c->bev.push_back(e);
+    }
+    CU(cudaEventRecord(c->bev[0], c->stream));
+    c->last_bands = sp.nbands;
     for (int64_t b = 0; b < sp.nbands; ++b) {
         const int64_t c0 = band_first_seg(sp, b), c1 = std::min(sp.nseg, c0 + sp.band_segs);
         int64_t vlo, vhi;
@@ -811,6 +820,7 @@ int stream_bands(dr_ctx* c, const StreamPlan& sp, const SumsArgs& base, int grid
         launch_fixup_range((int16_t*)c->dM.p, sp.u_dense, S, (const int32_t*)c->seg_off.p, (int32_t*)c->bckpt.p,
                            nwords_all, sp.dense_segs, c0, c1, c->sm_count * 16, c->stream, cword0);
         CU(cudaGetLastError());
+        CU(cudaEventRecord(c->bev[(size_t)(2 * b + 1)], c->stream));
         SumsArgs sa = base;
         sa.T.planes = (const ulonglong2*)c->bplanes.p;
         sa.T.ckpt = (const int32_t*)c->bckpt.p;
@@ -822,6 +832,7 @@ int stream_bands(dr_ctx* c, const StreamPlan& sp, const SumsArgs& base, int grid
                         scan_u64_tmp_elems(sa.n_slots), c->stream);
         launch_sums(sa, grid, 256, c->stream);
         CU(cudaGetLastError());
+        CU(cudaEventRecord(c->bev[(size_t)(2 * b + 2)], c->stream));
         *launches += 9;
     }
     return DR_OK;
@@ -895,6 +906,7 @@ int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq,
     if (!sq) return fail(DR_ERR_NOMEM, "internal: staging area too small");
     const void* sw = nullptr;
     c->wstage_used = 0;
+    c->last_bands = 0;
     if (!witems.empty()) {
         if (c->capturing) return fail(DR_ERR_ARG, "internal: windowed S1 under graph capture");
         if (c->wstage_cap < witems.size()) {  // the previous call's copy has completed (it synchronised)
@@ -1004,6 +1016,17 @@ int finish_queries(dr_ctx* c, const int64_t* X, int64_t nq, int launches, size_t
         st->plan_ms += elapsed_ms(c, 2, 3);
         st->sums_ms += elapsed_ms(c, 3, 4);
         st->d2h_ms += elapsed_ms(c, 4, 5);
+        for (int64_t b = 0; b < c->last_bands; ++b) {
+            float t = 0.f, u = 0.f;
+            if (cudaEventElapsedTime(&t, c->bev[(size_t)(2 * b)], c->bev[(size_t)(2 * b + 1)]) != cudaSuccess ||
+                cudaEventElapsedTime(&u, c->bev[(size_t)(2 * b + 1)], c->bev[(size_t)(2 * b + 2)]) != cudaSuccess) {
+                cudaGetLastError();  // timing is informational
+                t = u = 0.f;
+            }
+            st->band_table_ms += t;
+            st->band_sums_ms += u;
+        }
+        st->bands += c->last_bands;
         st->kernel_launches += launches;
         st->sieve_launches += 1;
         st->sums_launches += launches > 1 ? 1 : 0;
@@ -1170,6 +1193,7 @@ int dr_ctx_destroy(dr_ctx* c) {
     if (c->wstage) cudaFreeHost(c->wstage);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
+    for (auto& e : c->bev) cudaEventDestroy(e);
     if (c->side) {
         cudaStreamSynchronize(c->side);
         cudaStreamDestroy(c->side);

@@ -84,6 +84,9 @@ class Stats(ctypes.Structure):
         ("h2d_bytes", ctypes.c_uint64),
         ("d2h_bytes", ctypes.c_uint64),
         ("s1_comp_ops", ctypes.c_uint64),
+        ("band_table_ms", ctypes.c_double),
+        ("band_sums_ms", ctypes.c_double),
+        ("bands", ctypes.c_int64),
     ]
 
     def as_dict(self) -> dict:

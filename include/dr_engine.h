@@ -82,6 +82,9 @@ typedef struct {
     int32_t reserved;
     uint64_t h2d_bytes, d2h_bytes; /* host<->device bytes copied by the call   */
     uint64_t s1_comp_ops;    /* S1 lookups in the compressed tier (q > u_dense) */
+    double band_table_ms;    /* streamed table (both within sums_ms): device time of the */
+    double band_sums_ms;     /* bands' sieve + scan + fix-up, and of their S1 passes      */
+    int64_t bands;           /* bands streamed by the call (0: the table was held whole) */
 } dr_stats;
 
 typedef struct {
@@ -107,7 +110,8 @@ int dr_ctx_set_hbm_budget(dr_ctx *ctx, uint64_t bytes);
  * whose quotient falls in it are summed.  M(X) and the C/S1/S2 checksums are those
  * of the whole table.  Needs X > u_total and mu_limit <= u_res; batches never
  * stream.  u_resident = 0 (the default) holds every table whole.  The bands'
- * build and lookups count in dr_stats.sums_ms. */
+ * build and lookups count in dr_stats.sums_ms (split out in band_table_ms and
+ * band_sums_ms). */
 int dr_ctx_set_resident_limit(dr_ctx *ctx, int64_t u_resident, int64_t band_values);
 int dr_device_info(int device, int *sm_count, uint64_t *hbm_bytes);
 
