@@ -1516,6 +1516,13 @@ __global__ void __launch_bounds__(256, DRB_SUMS_MINB) sums_kernel(const SumsArgs
         const u64 want = total / (warps * 16) + 1;
         lg = 64 - __clzll(want);
         lg = max(11, min(lg, 16));
+        if (a.sparse) {
+            // a band pass of a streamed table: few ops per slot over every slot, and a
+            // warp visits a chunk's slots one after another (a dependent descriptor load
+            // each), so a chunk spans about 8 slots on average, however few its ops
+            const u64 per8 = 8 * total / max(a.n_slots, (u64)1) + 1;
+            lg = min(lg, 63 - __clzll(per8));
+        }
     }
     const u64 W = 1ull << lg;
     int cur_q = -1;

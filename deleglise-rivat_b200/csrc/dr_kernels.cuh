@@ -101,6 +101,7 @@ struct SumsArgs {
     u64* ticket;        // [0]: work-queue counter, [1]: error flag; zeroed before launch
     u64* acc;           // [3 * nq]: C, S1, S2
     int chunk_log2;     // 0: chosen on the device from the total
+    int sparse;         // a band pass of a streamed table (chunks sized by ops per slot)
     const double* rcp;       // rcp[n] = RN(1/n), 1 <= n <= inv_limit (< 2^32)
     i64 inv_limit;
     const double2* invw;     // invw[m] = {rcp(6m+1), rcp(6m+5)} with mu(j) in the low bits, m < invw_count
