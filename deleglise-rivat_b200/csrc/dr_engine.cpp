@@ -822,8 +822,6 @@ int stream_bands(dr_ctx* c, const StreamPlan& sp, const SumsArgs& base, int grid
         CU(cudaGetLastError());
         CU(cudaEventRecord(c->bev[(size_t)(2 * b + 1)], c->stream));
         SumsArgs sa = base;
-        sa.chunk_log2 = 0;
-        sa.sparse = 1;
         sa.T.planes = (const ulonglong2*)c->bplanes.p;
         sa.T.ckpt = (const int32_t*)c->bckpt.p;
         sa.T.cbase = cword0;
@@ -972,7 +970,6 @@ int enqueue_queries(dr_ctx* c, const int64_t* X, const dr_params* P, int64_t nq,
         sa.ticket = (u64*)c->ticket.p;
         sa.acc = (u64*)c->acc.p;
         sa.chunk_log2 = tuning ? tuning->chunk_log2 : 0;
-        sa.sparse = 0;
         sa.rcp = (const double*)c->inv.p;
         sa.inv_limit = inv_limit;
         sa.invw = (const double2*)c->invw.p;

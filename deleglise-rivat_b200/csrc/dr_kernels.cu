@@ -1000,12 +1000,27 @@ __global__ void plan_kernel(const QueryDev* __restrict__ qs, int nq, const Table
         const u64 s = s0 + (u64)lane;
         const bool valid = s < n_slots;
         const int qi = query_of_slot(qs, nq, valid ? s : n_slots - 1);
-        u64 v[6] = {0, 0, 0, 0, 0, 0};  // C, terms, evaluations, S1, S2, compressed S1
+        u64 v[7] = {0, 0, 0, 0, 0, 0, 0};  // C, terms, evaluations, S1, S2, compressed S1, S1 sum
         if (valid) {
             const QueryDev Q = qs[qi];
             const u64 local = s - Q.slot_base;
             EvalDesc d;
             decode_eval(Q, T, (i64)(local >> 1), (int)(local & 1), d, band);
+            if (band.s1_only && d.kind != EVAL_NONE && d.total <= kBandInThread) {
+                // a band pass: nearly every evaluation has a handful of lookups in the band;
+                // this thread sums them (exact quotients, the band's view of the table), so
+                // the sums kernel only walks the few evaluations with more
+                i64 part = 0;
+                for (int g = 0; g < kS1Seg; ++g) {
+                    i64 pg = 0;
+                    for (i64 i = 0; i < d.s1_cnt[g]; ++i)
+                        pg += table_M(T, udiv(d.y, s1_n_at(d.s1_n0[g], d.s1_stride[g], (u64)i)));
+                    part += d.coef * d.s1_sign[g] > 0 ? pg : -pg;
+                }
+                v[6] = (u64)part;
+                for (int g = 0; g < kS1Seg; ++g) d.s1_cnt[g] = 0;
+                d.total = 0;
+            }
             ops[s] = d.total;
             pack_slot(d, slots + s);
             if (wdesc && Q.win) {
@@ -1043,15 +1058,17 @@ __global__ void plan_kernel(const QueryDev* __restrict__ qs, int nq, const Table
         const int q0 = __shfl_sync(0xffffffffu, qi, 0);
         if (__all_sync(0xffffffffu, qi == q0)) {
 #pragma unroll
-            for (int i = 0; i < 6; ++i) v[i] = warp_sum_u64(v[i]);
+            for (int i = 0; i < 7; ++i) v[i] = warp_sum_u64(v[i]);
             if (lane == 0) {
                 atomicAdd(acc + 3 * qi, v[0]);
+                if (v[6]) atomicAdd(acc + 3 * qi + 1, v[6]);
                 unsigned long long* cq = reinterpret_cast<unsigned long long*>(counts + kCountsPerQuery * qi);
                 for (int i = 0; i < 5; ++i)
                     if (v[i + 1]) atomicAdd(cq + i, v[i + 1]);
             }
         } else if (valid) {
             if (v[0]) atomicAdd(acc + 3 * qi, v[0]);
+            if (v[6]) atomicAdd(acc + 3 * qi + 1, v[6]);
             unsigned long long* cq = reinterpret_cast<unsigned long long*>(counts + kCountsPerQuery * qi);
             for (int i = 0; i < 5; ++i)
                 if (v[i + 1]) atomicAdd(cq + i, v[i + 1]);
@@ -1516,13 +1533,6 @@ __global__ void __launch_bounds__(256, DRB_SUMS_MINB) sums_kernel(const SumsArgs
         const u64 want = total / (warps * 16) + 1;
         lg = 64 - __clzll(want);
         lg = max(11, min(lg, 16));
-        if (a.sparse) {
-            // a band pass of a streamed table: few ops per slot over every slot, and a
-            // warp visits a chunk's slots one after another (a dependent descriptor load
-            // each), so a chunk spans about 8 slots on average, however few its ops
-            const u64 per8 = 8 * total / max(a.n_slots, (u64)1) + 1;
-            lg = min(lg, 63 - __clzll(per8));
-        }
     }
     const u64 W = 1ull << lg;
     int cur_q = -1;
@@ -1536,7 +1546,10 @@ __global__ void __launch_bounds__(256, DRB_SUMS_MINB) sums_kernel(const SumsArgs
         const u64 o_end = min(o + W, total);
         u64 s = upper_slot(a.prefix, a.n_slots, o);
         while (o < o_end) {
-            while (a.prefix[s + 1] <= o) ++s;
+            // the next slot with ops: a few steps over slots without, then a search (a
+            // band pass of a streamed table leaves long runs of such slots)
+            for (int k = 0; k < 4 && a.prefix[s + 1] <= o; ++k) ++s;
+            if (a.prefix[s + 1] <= o) s = upper_slot(a.prefix, a.n_slots, o);
             const u64 sbase = a.prefix[s];
             const int qi = a.nq == 1 ? 0 : query_of_slot(a.queries, a.nq, s);
             __syncwarp();

@@ -101,7 +101,6 @@ struct SumsArgs {
     u64* ticket;        // [0]: work-queue counter, [1]: error flag; zeroed before launch
     u64* acc;           // [3 * nq]: C, S1, S2
     int chunk_log2;     // 0: chosen on the device from the total
-    int sparse;         // a band pass of a streamed table (chunks sized by ops per slot)
     const double* rcp;       // rcp[n] = RN(1/n), 1 <= n <= inv_limit (< 2^32)
     i64 inv_limit;
     const double2* invw;     // invw[m] = {rcp(6m+1), rcp(6m+5)} with mu(j) in the low bits, m < invw_count
@@ -157,6 +156,9 @@ void launch_fixup(int16_t* dM, i64 u_dense, int S, const int32_t* seg_off, int32
 // outer terms, evaluations, S1 lookups, S2 wheel positions, and the S1 lookups
 // whose quotient lies in the compressed tier (q > u_dense).
 constexpr int kCountsPerQuery = 5;
+// A band pass of a streamed table: evaluations with at most this many S1 lookups in the
+// band are summed by the planning thread itself (ops 0 for the sums kernel).
+constexpr int kBandInThread = 64;
 void launch_plan(const QueryDev* q, int nq, const TableView& T, u64 n_slots, u64* ops, u64* acc,
                  i64* counts, S1WinDesc* wdesc, SlotDesc* slots, int sm_count, cudaStream_t s,
                  const S1Band& band = S1Band{0, ~0ull, 0});
