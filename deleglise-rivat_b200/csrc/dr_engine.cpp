@@ -645,6 +645,33 @@ void band_values_of(const StreamPlan& sp, int64_t b, int64_t* vlo, int64_t* vhi)
     *vhi = std::min(sp.u_total, sp.u_dense + (c1 - sp.dense_segs) * sp.S);
 }
 
+// The bands of a table of ut values (dense tier ud, S-value segments) under a resident
+// limit: the resident part ends on a segment boundary of the whole table's layout, at
+// least one compressed segment above u_dense; sp->nbands == 0: nothing streams.
+void stream_geometry(int64_t ut, int64_t ud, int S, int64_t u_resident, int64_t band_values, StreamPlan* sp) {
+    *sp = StreamPlan{};
+    if (u_resident <= 0 || ut <= u_resident) return;
+    const int64_t res_segs = std::max<int64_t>(1, (u_resident - ud) / S);
+    if (ud + res_segs * S >= ut) return;
+    sp->S = S;
+    sp->u_total = ut;
+    sp->u_dense = ud;
+    sp->u_res = ud + res_segs * S;
+    sp->dense_segs = (ud + S - 1) / S;
+    sp->nseg = sp->dense_segs + (ut - ud + S - 1) / S;
+    sp->nseg_res = sp->dense_segs + res_segs;
+    sp->band_segs = band_values > 0 ? std::max<int64_t>(1, band_values / S) : res_segs;
+    sp->band_segs = std::min(sp->band_segs, sp->nseg - sp->nseg_res);
+    sp->nbands = (sp->nseg - sp->nseg_res + sp->band_segs - 1) / sp->band_segs;
+}
+
+// A band whose halves n/2 all lie in the resident compressed tier (vlo >= 2 u_dense, vhi
+// well below 2 u_res) can be sieved in odd mode, its even values' mu read from the
+// resident plane words (odd mode needs u_dense on a 64-value word).
+bool band_odd(const StreamPlan& sp, int64_t vlo, int64_t vhi) {
+    return sp.u_dense % 64 == 0 && vlo >= 2 * sp.u_dense && vhi + 2 * (int64_t)sp.S <= 2 * sp.u_res;
+}
+
 // Decide whether the query streams, and reserve every buffer the bands use before the
 // resident build (nothing may grow once launches are queued: the segment offsets of the
 // resident table carry into the first band).  *sp.nbands == 0: no streaming.
@@ -653,26 +680,12 @@ int plan_stream(dr_ctx* c, int64_t X, int64_t ut, int64_t ud, int64_t ml, const 
     if (c->u_resident <= 0 || ut <= c->u_resident) return DR_OK;
     if (X <= ut) return fail(DR_ERR_PARAMS, "a streamed table needs X > u_total (X = %lld, u_total = %lld)",
                              (long long)X, (long long)ut);
-    sp->S = pick_segment(&tune);
+    stream_geometry(ut, ud, pick_segment(&tune), c->u_resident, c->band_values, sp);
+    if (sp->nbands == 0) return DR_OK;
     const int64_t S = sp->S;
     sp->block = tune.block_threads ? tune.block_threads : 1024;
-    sp->u_total = ut;
-    sp->u_dense = ud;
     sp->mu_limit = ml;
-    // the resident part ends on a segment boundary of the whole table's layout
-    const int64_t res_segs = std::max<int64_t>(1, (c->u_resident - ud) / S);
-    sp->u_res = ud + res_segs * S;
-    if (sp->u_res >= ut) {
-        *sp = StreamPlan{};
-        return DR_OK;
-    }
     if (ml > sp->u_res) return fail(DR_ERR_PARAMS, "mu_limit %lld above the resident table", (long long)ml);
-    sp->dense_segs = (ud + S - 1) / S;
-    sp->nseg = sp->dense_segs + (ut - ud + S - 1) / S;
-    sp->nseg_res = sp->dense_segs + res_segs;
-    sp->band_segs = c->band_values > 0 ? std::max<int64_t>(1, c->band_values / S) : res_segs;
-    sp->band_segs = std::min(sp->band_segs, sp->nseg - sp->nseg_res);
-    sp->nbands = (sp->nseg - sp->nseg_res + sp->band_segs - 1) / sp->band_segs;
     const std::vector<uint32_t>& pr = primes_upto(c, isqrt_i64(ut));
     // squares above S go to per-band buckets (the resident build buckets its own)
     int k = 0;
@@ -770,9 +783,7 @@ int stream_bands(dr_ctx* c, const StreamPlan& sp, const SumsArgs& base, int grid
     sieve_kernel_attrs(smem_o, true, sp.block, &per_o);
     const int64_t sgrid = (int64_t)c->sm_count * std::max(per, 1);
     const int64_t sgrid_o = (int64_t)c->sm_count * std::max(per_o, 1);
-    // A band whose halves n/2 all lie in the resident compressed tier (vlo >= 2 u_dense,
-    // vhi well below 2 u_res) runs in odd mode: its even values take mu from the resident
-    // plane words of their halves (odd mode needs u_dense on a 64-value word).
+    // odd-mode arguments for the bands whose halves are resident (band_odd)
     SieveArgs ao = a;
     const bool odd_ok = sp.u_dense % 64 == 0;
     if (odd_ok && (rc = set_sieve_moduli(c, pr, S / 2, ao, c->items_odd))) return rc;
@@ -789,7 +800,7 @@ int stream_bands(dr_ctx* c, const StreamPlan& sp, const SumsArgs& base, int grid
         int64_t vlo, vhi;
         band_values_of(sp, b, &vlo, &vhi);
         const int64_t cword0 = (c0 - sp.dense_segs) * (S / 64);
-        const bool odd = odd_ok && vlo >= 2 * sp.u_dense && vhi + 2 * (int64_t)S <= 2 * sp.u_res;
+        const bool odd = band_odd(sp, vlo, vhi);
         SieveArgs& a = odd ? ao : af;
         a.seg_begin = c0;
         a.seg_end = c1;
@@ -1635,6 +1646,20 @@ int dr_debug_piece(dr_ctx* c, const int32_t* piece, const uint64_t* q, int64_t n
 
 int dr_debug_piece32(dr_ctx* c, const int32_t* piece, const uint64_t* q, int64_t n, int64_t* out) {
     return debug_piece(c, piece, q, n, out, 1);
+}
+
+int64_t dr_debug_stream_plan(int64_t u_total, int64_t u_dense, int32_t segment_log2, int64_t u_resident,
+                             int64_t band_values, int64_t* u_res, int64_t* out, int64_t cap) {
+    if (!u_res || (cap > 0 && !out) || segment_log2 < 12 || segment_log2 > 18 || u_dense < 0 || u_dense > u_total)
+        return DR_ERR_ARG;
+    StreamPlan sp;
+    stream_geometry(u_total, u_dense, 1 << segment_log2, u_resident, band_values, &sp);
+    *u_res = sp.nbands ? sp.u_res : u_total;
+    for (int64_t b = 0; b < sp.nbands && b < cap; ++b) {
+        band_values_of(sp, b, out + 3 * b, out + 3 * b + 1);
+        out[3 * b + 2] = band_odd(sp, out[3 * b], out[3 * b + 1]) ? 1 : 0;
+    }
+    return sp.nbands;
 }
 
 int64_t dr_debug_sieve_plan(int64_t u_total, int64_t u_dense, int32_t segment_log2, int64_t first_wave,

@@ -165,6 +165,7 @@ def lib():
             "dr_tuner_propose": (i32, [vp, i64, u64, i32, i32, P, ctypes.POINTER(i32)]),
             "dr_measure_peaks": (i32, [i32, ctypes.POINTER(Peaks)]),
             "dr_debug_sieve_plan": (i64, [i64, i64, i32, i64, ctypes.POINTER(i64), i64]),
+            "dr_debug_stream_plan": (i64, [i64, i64, i32, i64, i64, ctypes.POINTER(i64), ctypes.POINTER(i64), i64]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -186,7 +187,7 @@ def exported_symbols() -> list:
         "dr_table_build_noalloc", "dr_autotune_batch",
         "dr_mlp_create", "dr_mlp_destroy", "dr_mlp_num_params", "dr_mlp_set_weights", "dr_mlp_get_weights",
         "dr_mlp_forward", "dr_mlp_grad", "dr_mlp_train", "dr_tuner_features", "dr_tuner_params", "dr_tuner_propose",
-        "dr_measure_peaks", "dr_debug_sieve_plan",
+        "dr_measure_peaks", "dr_debug_sieve_plan", "dr_debug_stream_plan",
     ]
 
 
@@ -204,6 +205,19 @@ def sieve_plan(u_total: int, u_dense: int, segment_log2: int, first_wave: int) -
     buf = (ctypes.c_int64 * (3 * max(n, 1)))()
     lib().dr_debug_sieve_plan(int(u_total), int(u_dense), int(segment_log2), int(first_wave), buf, n)
     return [(buf[3 * i], buf[3 * i + 1], bool(buf[3 * i + 2])) for i in range(n)]
+
+
+def stream_plan(u_total: int, u_dense: int, segment_log2: int, u_resident: int, band_values: int = 0):
+    """The bands of a streamed table: (u_res, [(vlo, vhi, odd mode), ...]); no bands when
+    nothing streams."""
+    ures = ctypes.c_int64()
+    args = (int(u_total), int(u_dense), int(segment_log2), int(u_resident), int(band_values), ctypes.byref(ures))
+    n = int(lib().dr_debug_stream_plan(*args, None, 0))
+    if n < 0:
+        _check(n)
+    buf = (ctypes.c_int64 * (3 * max(n, 1)))()
+    lib().dr_debug_stream_plan(*args, buf, n)
+    return ures.value, [(buf[3 * i], buf[3 * i + 1], bool(buf[3 * i + 2])) for i in range(n)]
 
 
 def measure_peaks(device: int = 0) -> dict:

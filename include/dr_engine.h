@@ -214,6 +214,13 @@ int dr_debug_piece32(dr_ctx *ctx, const int32_t *piece, const uint64_t *q, int64
  * DR_ERR_* code.  Needs no GPU. */
 int64_t dr_debug_sieve_plan(int64_t u_total, int64_t u_dense, int32_t segment_log2, int64_t first_wave,
                             int64_t *out, int64_t cap);
+/* The bands a streamed table (dr_ctx_set_resident_limit) of these limits would use --
+ * test support, no counterpart in the reference: *u_res = the resident part's end
+ * (u_total when nothing streams), then per band {vlo, vhi, odd}: its values (vlo, vhi]
+ * and whether it is sieved in odd mode.  Writes at most cap triples; returns the band
+ * count (0: nothing streams) or a negative DR_ERR_* code.  Needs no GPU. */
+int64_t dr_debug_stream_plan(int64_t u_total, int64_t u_dense, int32_t segment_log2, int64_t u_resident,
+                             int64_t band_values, int64_t *u_res, int64_t *out, int64_t cap);
 
 /* Measured throughput ceilings of the units this engine's kernels are bound by
  * (measurement support for bench.py; no counterpart in the reference).  Each is
