@@ -676,16 +676,20 @@ bool band_odd(const StreamPlan& sp, int64_t vlo, int64_t vhi) {
 // resident build (nothing may grow once launches are queued: the segment offsets of the
 // resident table carry into the first band).  *sp.nbands == 0: no streaming.
 int plan_stream(dr_ctx* c, int64_t X, int64_t ut, int64_t ud, int64_t ml, const dr_params& tune, StreamPlan* sp) {
-    *sp = StreamPlan{};
-    if (c->u_resident <= 0 || ut <= c->u_resident) return DR_OK;
-    if (X <= ut) return fail(DR_ERR_PARAMS, "a streamed table needs X > u_total (X = %lld, u_total = %lld)",
-                             (long long)X, (long long)ut);
     stream_geometry(ut, ud, pick_segment(&tune), c->u_resident, c->band_values, sp);
     if (sp->nbands == 0) return DR_OK;
+    if (X <= ut) {
+        *sp = StreamPlan{};
+        return fail(DR_ERR_PARAMS, "a streamed table needs X > u_total (X = %lld, u_total = %lld)", (long long)X,
+                    (long long)ut);
+    }
     const int64_t S = sp->S;
     sp->block = tune.block_threads ? tune.block_threads : 1024;
     sp->mu_limit = ml;
-    if (ml > sp->u_res) return fail(DR_ERR_PARAMS, "mu_limit %lld above the resident table", (long long)ml);
+    if (ml > sp->u_res) {
+        *sp = StreamPlan{};
+        return fail(DR_ERR_PARAMS, "mu_limit %lld above the resident table", (long long)ml);
+    }
     const std::vector<uint32_t>& pr = primes_upto(c, isqrt_i64(ut));
     // squares above S go to per-band buckets (the resident build buckets its own)
     int k = 0;
@@ -746,8 +750,7 @@ int stream_bands(dr_ctx* c, const StreamPlan& sp, const SumsArgs& base, int grid
     const int S = sp.S;
     int lgS = 0;
     while ((1 << lgS) < S) ++lgS;
-    SieveArgs af;
-    SieveArgs& a = af;  // full-mode arguments
+    SieveArgs a;  // full-mode arguments (ao: odd mode)
     a.u_total = sp.u_total;
     a.u_dense = sp.u_dense;
     a.mu_limit = sp.mu_limit;
@@ -801,31 +804,31 @@ int stream_bands(dr_ctx* c, const StreamPlan& sp, const SumsArgs& base, int grid
         band_values_of(sp, b, &vlo, &vhi);
         const int64_t cword0 = (c0 - sp.dense_segs) * (S / 64);
         const bool odd = band_odd(sp, vlo, vhi);
-        SieveArgs& a = odd ? ao : af;
-        a.seg_begin = c0;
-        a.seg_end = c1;
-        a.cword0 = cword0;
-        a.sq_off = nullptr;
-        a.sq_pos = nullptr;
-        a.sq_seg0 = c0;
-        a.sqC_first = sqC;
+        SieveArgs& m = odd ? ao : a;
+        m.seg_begin = c0;
+        m.seg_end = c1;
+        m.cword0 = cword0;
+        m.sq_off = nullptr;
+        m.sq_pos = nullptr;
+        m.sq_seg0 = c0;
+        m.sqC_first = sqC;
         if (sp.band_sq[(size_t)b] > 0 && sqC < (int)np) {
             const u64 nb = (u64)(c1 - c0);
             CU(cudaMemsetAsync(c->sq_cnt.p, 0, nb * 8, c->stream));
             CU(cudaMemsetAsync(c->sq_cur.p, 0, nb * 8, c->stream));
-            launch_sq_bucket_count(a.primes, a.sqC_first, (int)np, vlo, vhi, sp.u_dense, sp.dense_segs, lgS, c0,
+            launch_sq_bucket_count(m.primes, m.sqC_first, (int)np, vlo, vhi, sp.u_dense, sp.dense_segs, lgS, c0,
                                    (u64*)c->sq_cnt.p, c->stream);
             launch_scan_u64((const u64*)c->sq_cnt.p, (u64*)c->sq_off.p, nb, (u64*)c->sq_tmp.p,
                             scan_u64_tmp_elems(nb), c->stream);
-            launch_sq_bucket_fill(a.primes, a.sqC_first, (int)np, vlo, vhi, sp.u_dense, sp.dense_segs, lgS, c0,
+            launch_sq_bucket_fill(m.primes, m.sqC_first, (int)np, vlo, vhi, sp.u_dense, sp.dense_segs, lgS, c0,
                                   (const u64*)c->sq_off.p, (u64*)c->sq_cur.p, (uint32_t*)c->sq_pos.p, c->stream);
-            a.sq_off = (const u64*)c->sq_off.p;
-            a.sq_pos = (const uint32_t*)c->sq_pos.p;
+            m.sq_off = (const u64*)c->sq_off.p;
+            m.sq_pos = (const uint32_t*)c->sq_pos.p;
             *launches += 5;
         } else {
-            a.sqC_first = (int)np;  // no bucketed hit in this band: squares thread-per-prime
+            m.sqC_first = (int)np;  // no bucketed hit in this band: squares thread-per-prime
         }
-        launch_sieve(a, odd, (int)std::max<int64_t>(1, std::min<int64_t>(c1 - c0, odd ? sgrid_o : sgrid)), sp.block,
+        launch_sieve(m, odd, (int)std::max<int64_t>(1, std::min<int64_t>(c1 - c0, odd ? sgrid_o : sgrid)), sp.block,
                      odd ? smem_o : smem, c->stream);
         launch_seg_scan_range((const int32_t*)c->seg_sum.p, (int32_t*)c->seg_off.p, c0, c1, 1024, c->stream);
         launch_fixup_range((int16_t*)c->dM.p, sp.u_dense, S, (const int32_t*)c->seg_off.p, (int32_t*)c->bckpt.p,
