@@ -23,6 +23,10 @@ on this GPU by dr_measure_peaks), `default_params` and `learned_tuner` (the
 same step with the reference's parameters and with the learned tuner's
 proposal) and `batched` (the 256-query batch: replay throughput, first-call
 cost, launches per batch).
+
+Profiling cases: `--x X` times M(X) instead of M(10^16), `--u U` sets the table
+size, and `--resident R --band B` streams the table above R values in bands of B
+(the line then carries `stream` and the bands' share of the sums phase).
 """
 from __future__ import annotations
 
